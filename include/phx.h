@@ -1,0 +1,179 @@
+/*
+ * phx.h -- C ABI of the B200 time-stepping library for the driven-dissipative
+ * Gross-Pitaevskii equation with reservoir (the PHOENIX RK hot path).
+ *
+ * The reference has no library API: its plug-in point is the C++ class
+ * `PHOENIX::Solver` (include/solver/solver.hpp:22-170) selected by string
+ * through `SolverFactory` / `REGISTER_SOLVER` (include/solver/solver_factory.hpp:31-84),
+ * fed by `SystemParameters` (include/system/system_parameters.hpp:22-131) and
+ * reached from the CLI (source/main.cu:46-135) or by pyphoenix as a
+ * subprocess (pyphoenix/pyphoenix.py:162-216).  Each entry point below
+ * names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every call returns phx_status; no exception, exit() or abort() crosses
+ *    the ABI.  phx_last_error() gives a message for the last failure.
+ *  - A handle owns all of its device memory.  Host pointers passed in are
+ *    borrowed for the duration of the call only.
+ *  - A handle is not thread safe; distinct handles are independent.  All of
+ *    a handle's GPU work is ordered on its stream.
+ *  - Grids are N_r rows x N_c columns, row-major with the column index
+ *    fastest (the reference's full-grid order, index = row * N_c + col).
+ *    Complex values are interleaved (re, im).
+ */
+#ifndef PHX_H
+#define PHX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHX_ABI_VERSION 1
+
+typedef enum {
+    PHX_OK = 0,
+    PHX_ERR_INVALID_ARG = 1,  /* bad size, pointer, enum or parameter      */
+    PHX_ERR_OOM = 2,          /* device or host allocation failed          */
+    PHX_ERR_CUDA = 3,         /* a CUDA / cuFFT call failed                 */
+    PHX_ERR_NONFINITE = 4,    /* NaN or Inf found in a reduction            */
+    PHX_ERR_TIMEOUT = 5,      /* a bounded wait gave up                     */
+    PHX_ERR_UNSUPPORTED = 6,  /* valid request this build does not support  */
+    PHX_ERR_STATE = 7         /* call not valid in the handle's state       */
+} phx_status;
+
+typedef enum { PHX_F32 = 0, PHX_F64 = 1 } phx_dtype;
+
+/* iterator keys of REGISTER_SOLVER: "RK4" (runge_kutta.cu:96), "DP45" (dormand_prince.cu:97) */
+typedef enum { PHX_ITER_RK4 = 0, PHX_ITER_DP45 = 1 } phx_iterator;
+
+/* DP45 error norm.  PHX_NORM_REFERENCE reproduces the reference's sums over
+ * halo-padded subgrids of a single subgrid (cuda_matrix.cuh:614-632,699-705,
+ * solver.cu:73-75); PHX_NORM_INTERIOR sums over grid points only. */
+typedef enum { PHX_NORM_REFERENCE = 0, PHX_NORM_INTERIOR = 1 } phx_norm_mode;
+
+/* Fields of MatrixContainer (include/solver/matrix_container.cuh:16-53) that
+ * are inputs or state of the iteration. */
+typedef enum {
+    PHX_PSI_PLUS = 0,        /* wavefunction_plus   complex          */
+    PHX_PSI_MINUS = 1,       /* wavefunction_minus  complex (TE/TM)  */
+    PHX_N_PLUS = 2,          /* reservoir_plus      real             */
+    PHX_N_MINUS = 3,         /* reservoir_minus     real (TE/TM)     */
+    PHX_PUMP_PLUS = 4,       /* pump_plus           real, per group  */
+    PHX_PUMP_MINUS = 5,      /* pump_minus          real, per group  */
+    PHX_POTENTIAL_PLUS = 6,  /* potential_plus      real, per group  */
+    PHX_POTENTIAL_MINUS = 7, /* potential_minus     real, per group  */
+    PHX_PULSE_PLUS = 8,      /* pulse_plus          complex, per group */
+    PHX_PULSE_MINUS = 9,     /* pulse_minus         complex, per group */
+    PHX_FFT_MASK_PLUS = 10,  /* fft_mask_plus       real, real-space order */
+    PHX_FFT_MASK_MINUS = 11  /* fft_mask_minus      real, real-space order */
+} phx_field;
+
+/* Temporal envelope kinds (include/system/envelope.hpp:63-69,165-175) */
+typedef enum { PHX_TEMPORAL_CONSTANT = 0, PHX_TEMPORAL_IEXP = 1, PHX_TEMPORAL_COS = 2, PHX_TEMPORAL_GAUSS = 3 } phx_temporal_kind;
+
+/* Which temporal-envelope family a group belongs to */
+typedef enum { PHX_ENV_PUMP = 0, PHX_ENV_POTENTIAL = 1, PHX_ENV_PULSE = 2 } phx_envelope;
+
+/* Replaces SystemParameters (system_parameters.hpp:22-131) for the
+ * iteration: the physics and numerics flags of system_initialization.cpp:13-261
+ * after calculateAuto (system.cpp:116-160).  h_bar_s and m_eff are the
+ * scaled values (--hbarscaled, --meff); the library derives dx = L/(N-1),
+ * dV, 1/dx^2, -2(1/dx^2+1/dy^2), -hbar^2/2m and 1/hbar exactly as
+ * calculateAuto does in the chosen precision. */
+typedef struct {
+    int32_t abi_version; /* PHX_ABI_VERSION */
+    int32_t N_c, N_r;
+    double L_x, L_y;
+    double h_bar_s, m_eff;
+    double gamma_c, gamma_r, g_c, g_r, R, g_pm, delta_LT;
+    int32_t periodic_x, periodic_y; /* --boundary; 0 = zero (reference default) */
+    int32_t tetm;                   /* -tetm */
+    int32_t use_reservoir;          /* reservoir present (pump or initReservoir, not -noReservoir) */
+    int32_t dtype;                  /* phx_dtype: the build precision of the reference */
+    int32_t iterator;               /* phx_iterator */
+    int32_t adaptive;               /* -adaptive (DP45) */
+    int32_t norm_mode;              /* phx_norm_mode (DP45 only) */
+    double dt, t0, t_max;           /* --dt, --t0, --tmax */
+    double tol, dt_min, dt_max;     /* --tol, --rkvdt */
+    double fft_every;               /* --fftEvery (ps) */
+    double stochastic_amplitude;    /* --dw ; 0 = deterministic */
+    uint64_t seed;                  /* noise seed */
+    int32_t n_pump_groups, n_potential_groups, n_pulse_groups;
+    int32_t device;                 /* CUDA device ordinal */
+} phx_params;
+
+typedef struct {
+    double t, dt;                   /* simulated time and current dt after the call */
+    int64_t iterations;             /* Solver::iterate calls made by this call */
+    int64_t accepted, rejected;     /* DP45 attempts */
+    int64_t fft_filters;            /* k-space mask applications */
+    int64_t kernel_launches;        /* this library's kernels launched */
+} phx_step_info;
+
+typedef struct phx_handle phx_handle;
+
+/* Replaces SolverFactory::create + Solver::initialize (solver_factory.hpp:53-60,
+ * solver_initialization.cu:13-35): allocate and zero all state for `p`. */
+phx_status phx_create(const phx_params* p, phx_handle** out);
+
+/* Frees every device buffer and stream of the handle (no reference
+ * counterpart: the reference never frees).  NULL is accepted. */
+phx_status phx_destroy(phx_handle* h);
+
+/* Replaces the host->device upload of one matrix
+ * (initializeMatricesFromSystem, solver_initialization.cu:37-174, and
+ * CUDAMatrix::hostToDeviceSync, cuda_matrix.cuh:281-306).  `host` holds
+ * count = N_c*N_r values (complex fields: 2*N_c*N_r reals) of type
+ * host_dtype; group selects the temporal group of pump/potential/pulse. */
+phx_status phx_set_field(phx_handle* h, int32_t field, int32_t group, const void* host, int64_t count, int32_t host_dtype);
+
+/* Replaces CUDAMatrix::getFullMatrix (device->host, cuda_matrix.cuh:375-403,
+ * used by outputMatrices, solver_output_matrices.cu:20-70). */
+phx_status phx_get_field(phx_handle* h, int32_t field, int32_t group, void* host, int64_t count, int32_t host_dtype);
+
+/* Replaces Envelope::addTemporal (envelope.cpp:88-120) for one group. */
+phx_status phx_set_temporal(phx_handle* h, int32_t envelope, int32_t group, int32_t kind, double t0, double sigma,
+                            double freq);
+
+/* Replaces the main loop's calls of Solver::iterate (main.cu:80-117,
+ * solver.cu:22-70): run iterate() until t >= t_max or max_iterations calls. */
+phx_status phx_step(phx_handle* h, int64_t max_iterations, phx_step_info* info);
+
+/* Current t and dt (SystemParameters::p.t / p.dt). */
+phx_status phx_get_time(phx_handle* h, double* t, double* dt);
+
+/* Overwrite t and dt (--t0 / --dt, and the main loop's last-step dt
+ * adjustment, main.cu:86-101). */
+phx_status phx_set_time(phx_handle* h, double t, double dt);
+
+/* Sum over grid points of |field|^2 accumulated in FP64 (the reference's
+ * transformReduce with transform_abs2, cuda_matrix.cuh:614-632, without
+ * halo cells).  Real fields sum their squares. */
+phx_status phx_sum_abs2(phx_handle* h, int32_t field, double* out);
+
+/* Borrow the device pointer of a field for zero-copy interop (e.g. torch):
+ * pointer to grid point (0,0), row pitch in elements.  Valid until the
+ * handle is destroyed; the caller must order its own work on the handle's
+ * stream (phx_get_stream). */
+phx_status phx_field_device_ptr(phx_handle* h, int32_t field, int32_t group, void** dev_ptr, int64_t* row_pitch_elems);
+
+/* The handle's cudaStream_t, as void*. */
+phx_status phx_get_stream(phx_handle* h, void** stream);
+
+/* Message of the last failed call on this handle (or of the last failed
+ * phx_create in this thread when h is NULL). */
+const char* phx_last_error(const phx_handle* h);
+
+const char* phx_status_string(int32_t status);
+
+/* ABI version and build description ("sm_100a ..."). */
+int32_t phx_abi_version(void);
+const char* phx_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

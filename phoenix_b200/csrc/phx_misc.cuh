@@ -1,0 +1,154 @@
+// Small kernels around the stage kernels: ring maintenance of padded planes,
+// the k-space mask filter's gather / mask / scatter passes, and the final
+// FP64 reduction of per-block partial sums.
+#pragma once
+
+#include "phx_device.cuh"
+
+namespace phx {
+
+// Zero the ring of a padded plane along non-periodic axes (what
+// synchronize_halos does for a zero boundary, kernel_halo.cuh:68-70) and
+// write ring-1 periodic images along periodic axes.  Grid-stride over the
+// ring cells only: top/bottom bands of G rows (full padded width) and
+// left/right bands of G columns (interior rows).
+template <typename V>
+__global__ void ring_fill_kernel(V* base, int N_r, int N_c, long long pitch, int G, int periodic_x, int periodic_y) {
+    const long long W = N_c + 2LL * G;
+    const long long band_tb = (long long)G * W;      // one of top / bottom
+    const long long band_lr = (long long)N_r * G;    // one of left / right
+    const long long total = 2 * band_tb + 2 * band_lr;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int r, c;
+        if (t < 2 * band_tb) {
+            const long long u = t % band_tb;
+            const int rr = (int)(u / W);
+            c = (int)(u % W) - G;
+            r = t < band_tb ? -G + rr : N_r + rr;
+        } else {
+            const long long u = (t - 2 * band_tb) % band_lr;
+            r = (int)(u / G);
+            const int cc = (int)(u % G);
+            c = (t - 2 * band_tb) < band_lr ? -G + cc : N_c + cc;
+        }
+        const bool out_r = r < 0 || r >= N_r;
+        const bool out_c = c < 0 || c >= N_c;
+        bool zero = (out_r && !periodic_y) || (out_c && !periodic_x);
+        V v{};
+        if (!zero) {
+            // periodic image; only ring 1 is ever read by the stencil, deeper
+            // rings along periodic axes are filled with images as well.
+            const int sr = out_r ? (r + N_r) % N_r : r;
+            const int sc = out_c ? (c + N_c) % N_c : c;
+            v = base[(long long)sr * pitch + sc];
+        }
+        base[(long long)r * pitch + c] = v;
+    }
+}
+
+// padded interior -> contiguous N_r x N_c (full_grid layout, index r*N_c + c)
+template <typename T>
+__global__ void gather_interior_kernel(const cx<T>* __restrict__ src, long long pitch, int N_r, int N_c, cx<T>* __restrict__ dst) {
+    const long long n = (long long)N_r * N_c;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / N_c), c = (int)(i % N_c);
+        dst[i] = src[(long long)r * pitch + c];
+    }
+}
+
+// kernel_mask_fft (kernel_fft.cuh:35-39): data = data / N * mask
+template <typename T>
+__global__ void mask_kernel(cx<T>* __restrict__ data, const T* __restrict__ mask, long long n) {
+    const T fn = (T)n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const cx<T> d = data[i];
+        const T m = mask[i];
+        data[i] = mk(rmul(rdiv(d.re, fn), m), rmul(rdiv(d.im, fn), m));
+    }
+}
+
+// contiguous -> padded interior, plus ring-1 periodic images
+template <typename T>
+__global__ void scatter_interior_kernel(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, long long pitch, int N_r,
+                                        int N_c, int periodic_x, int periodic_y) {
+    const long long n = (long long)N_r * N_c;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / N_c), c = (int)(i % N_c);
+        const cx<T> v = src[i];
+        dst[(long long)r * pitch + c] = v;
+        const bool ex = periodic_x && (c == 0 || c == N_c - 1);
+        const bool ey = periodic_y && (r == 0 || r == N_r - 1);
+        const int ci = c == 0 ? N_c : -1;
+        const int ri = r == 0 ? N_r : -1;
+        if (ex) dst[(long long)r * pitch + ci] = v;
+        if (ey) dst[(long long)ri * pitch + c] = v;
+        if (ex && ey) dst[(long long)ri * pitch + ci] = v;
+    }
+}
+
+// Sum of n (error, norm) pairs in a fixed order: one block, deterministic.
+__global__ void finalize_pairs_kernel(const double* __restrict__ partials, long long n, double* __restrict__ out) {
+    __shared__ double sa[32], sb[32];
+    double a = 0.0, b = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        a += partials[2 * i];
+        b += partials[2 * i + 1];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sa[warp] = a;
+        sb[warp] = b;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) / 32;
+        a = lane < nw ? sa[lane] : 0.0;
+        b = lane < nw ? sb[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) {
+            out[0] = a;
+            out[1] = b;
+        }
+    }
+}
+
+// Sum over interior points of |z|^2 (complex) or x^2 (real), FP64, two-pass:
+// per-block partials (second slot unused) then finalize_pairs_kernel.
+template <typename T, bool COMPLEX>
+__global__ void sum_abs2_kernel(const T* __restrict__ base, long long pitch, int N_r, int N_c, double* __restrict__ partials) {
+    double a = 0.0;
+    const long long n = (long long)N_r * N_c;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / N_c), c = (int)(i % N_c);
+        if (COMPLEX) {
+            const T re = base[2 * ((long long)r * pitch + c)], im = base[2 * ((long long)r * pitch + c) + 1];
+            a += (double)re * (double)re + (double)im * (double)im;
+        } else {
+            const T x = base[(long long)r * pitch + c];
+            a += (double)x * (double)x;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    __shared__ double s[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s[warp] = a;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) / 32;
+        a = lane < nw ? s[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) {
+            partials[2 * blockIdx.x] = a;
+            partials[2 * blockIdx.x + 1] = 0.0;
+        }
+    }
+}
+
+}  // namespace phx
