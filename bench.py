@@ -1,0 +1,401 @@
+"""Benchmark: microseconds per RK4 iteration of the scalar polariton GP equation
+with reservoir on a 1024 x 1024 grid (FP32 by default), one replica per GPU.
+
+Workload (synthetic, seeded): 1024^2 periodic box of 100 um, hbar = 0.6582 meV ps,
+m_eff = 5.6e-4 m_e (3.1840 meV ps^2/um^2), gamma_c 0.15/ps, gamma_r 0.225/ps,
+g_c 6e-6, g_r 1.2e-5 meV um^2, R 0.01 ps^-1 um^2, dt 0.02 ps; Gaussian pump of
+width 10 um at 1.5x threshold; disorder potential (white noise smoothed to
+1 um correlation, 0.1 meV rms); k-space super-Gaussian mask (order 4, cutoff
+0.8 k_max) applied every 100 iterations; psi0 complex white noise of
+amplitude 1e-2, n0 = 0.
+
+Legs of the JSON line:
+  value      device time per iteration (CUDA events on the solver's stream),
+             L2 flushed (256 MiB write) between timed iterations, max over ranks
+  e2e        the same workload through the public API with host buffers:
+             upload psi0/n0, run in chunks of 100 iterations reading the FP64
+             norm back after each chunk, download psi and n at the end
+  roofline   the dominant kernel (fused RK4 stage 2/3) from per-launch CUDA
+             events recorded by the library on its stream during the timed
+             region: algorithmic bytes / average duration vs measured HBM peak
+  cpu_baseline  the reference's CPU build (PHOENIX compiled from its sources,
+             oracle/_ref) on a bounded sample of the same workload, all host cores
+`--impl reference` runs that reference CPU build alone (rank 0 of any launch).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 1024
+L_BOX = 100.0
+PHYS = dict(h_bar_s=0.6582, m_eff=3.1840, gamma_c=0.15, gamma_r=0.225, g_c=6e-6, g_r=1.2e-5, R=0.01)
+DT = 0.02
+MASK_EVERY = 100
+P_TH = 0.15 * 0.225 / 0.01
+METRIC = "us_per_rk4_iteration_1024x1024"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+
+
+def workload(n, seed=2):
+    rng = np.random.default_rng(seed)
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n)
+    X, Y = np.meshgrid(x, x)
+    psi0 = 1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    pump = 1.5 * P_TH * np.exp(-(X ** 2 + Y ** 2) / (2 * 10.0 ** 2))
+    noise = np.random.default_rng(3).standard_normal((n, n))
+    k = 2 * np.pi * np.fft.fftfreq(n, d=L_BOX / (n - 1))
+    KX, KY = np.meshgrid(k, k)
+    pot = np.real(np.fft.ifft2(np.fft.fft2(noise) * np.exp(-(KX ** 2 + KY ** 2) * 1.0 ** 2 / 2)))
+    pot *= 0.1 / np.sqrt(np.mean(pot ** 2))
+    loc = -1.0 + 2.0 * np.arange(n) / (n - 1)
+    LX, LY = np.meshgrid(loc, loc)
+    mask = np.exp(-((0.5 * ((LX / 0.8) ** 2 + (LY / 0.8) ** 2)) ** 4))
+    return dict(psi0=psi0, pump=pump, potential=pot, mask=mask)
+
+
+def system(pb, n, dtype, device):
+    return pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                               periodic_boundary_y=True, dtype=dtype, iterator="RK4", dt=DT, t0=0.0, t_max=1e12,
+                               fft_every=MASK_EVERY * DT * (1 - 1e-6), pump_temporal=[pb.Temporal()],
+                               potential_temporal=[pb.Temporal()], device=device)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
+                                          "100", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def write_txt(path, arr, digits=9):
+    arr = np.asarray(arr)
+    n_r, n_c = arr.shape
+    with open(path, "w") as f:
+        f.write(f"# SIZE {n_c} {n_r} {L_BOX} {L_BOX} {L_BOX / (n_c - 1)} {L_BOX / (n_r - 1)} :: PHOENIX_ MATRIX\n")
+        np.savetxt(f, np.real(arr), fmt=f"%.{digits}g")
+        if np.iscomplexobj(arr):
+            np.savetxt(f, np.imag(arr), fmt=f"%.{digits}g")
+
+
+def reference_cpu_run(n, dtype, iters, wl):
+    """Run the reference CPU build (all host cores) for `iters` RK4 iterations of
+    the workload; returns (us_per_iteration, cores, binary) or None."""
+    variant = "fp32" if dtype == "f32" else "fp64"
+    cand = [os.path.join(REF_BIN, f"phoenix_cpu_{variant}_v3"), os.path.join(REF_BIN, f"phoenix_cpu_{variant}")]
+    binary = next((b for b in cand if os.path.exists(b)), None)
+    if binary is None:
+        return None
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as tmp:
+        files = {}
+        for key in ("psi0", "pump", "potential", "mask"):
+            files[key] = os.path.join(tmp, key + ".txt")
+            write_txt(files[key], wl[key])
+        t_max = iters * DT * (1 - 1e-9)
+        args = [binary, "--N", str(n), str(n), "--L", str(L_BOX), str(L_BOX), "--dt", str(DT), "--tmax", repr(t_max),
+                "--outEvery", "1e9", "--output", "none", "--path", os.path.join(tmp, "out"), "--threads", str(cores),
+                "--boundary", "periodic", "periodic", "--hbarscaled", str(PHYS["h_bar_s"]), "--meff",
+                str(PHYS["m_eff"]), "--gammaC", str(PHYS["gamma_c"]), "--gammaR", str(PHYS["gamma_r"]), "--gc",
+                str(PHYS["g_c"]), "--gr", str(PHYS["g_r"]), "--R", str(PHYS["R"]), "--fftEvery",
+                repr(MASK_EVERY * DT * (1 - 1e-6)), "--initState", "load", files["psi0"], "1", "add", "both",
+                "--pump", "load", files["pump"], "1", "add", "both", "--potential", "load", files["potential"], "1",
+                "add", "both", "--fftMask", "load", files["mask"], "1", "add", "both"]
+        proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
+        m = re.search(r"-->\s*([0-9.eE+-]+)\s*mus/it", proc.stdout)
+        if proc.returncode != 0 or not m:
+            return None
+        return float(m.group(1)), cores, os.path.basename(binary)
+
+
+def oracle_port_run(n, dtype, iters, wl):
+    """Fallback CPU baseline: the C restatement (single thread)."""
+    from oracle import phx_oracle as O
+
+    case = dict(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, g_pm=0.0, delta_LT=0.0, dtype=dtype, iterator="RK4",
+                dt=DT, t_max=1e12, periodic_x=1, periodic_y=1, pumps=[(0, 0, 0)], potentials=[0.0],
+                mask_cut=0.8, fft_every=MASK_EVERY * DT * (1 - 1e-6))
+    fields = {"psi_plus": wl["psi0"], "pump_0": wl["pump"], "potential_0": wl["potential"], "fft_mask": wl["mask"]}
+    t0 = time.perf_counter()
+    O.run(case, fields, max_steps=iters)
+    return (time.perf_counter() - t0) / iters * 1e6, 1, "oracle/phx_oracle.c"
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = args.n
+    wl = workload(n)
+    iters = max(3, min(args.steps + args.warmup, args.ref_iters))
+    res = reference_cpu_run(n, args.dtype, iters, wl)
+    kind = "reference"
+    if res is None:
+        res = oracle_port_run(n, args.dtype, max(2, iters // 20), wl)
+        kind = "port"
+    us, cores, what = res
+    line = {"metric": METRIC, "value": us, "unit": "us/iter", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": us / 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": config_dict(args),
+            "cpu_baseline": {"value": us, "unit": "us/iter", "cores": cores, "kind": kind,
+                             "sample": f"{iters} RK4 iterations of the {n}^2 workload with {what}"},
+            "e2e": {"value": us, "unit": "us/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def config_dict(args):
+    return {"workload": f"rk4_scalar_reservoir_pump_potential_mask_{args.n}x{args.n}_{args.dtype}",
+            "grid": [args.n, args.n], "iterator": "RK4", "boundary": "periodic", "dt_ps": DT,
+            "mask_every_iterations": MASK_EVERY, "physics": "polariton GP + reservoir, meV/ps/um, hbar 0.6582, "
+            "m_eff 5.6e-4 m_e", "replicas": "one independent simulation per GPU",
+            "l2": "256 MiB write between timed iterations (value); e2e runs back to back"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="phx", choices=["phx", "reference"])
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--ref-iters", type=int, default=400, help="cap on reference CPU iterations")
+    ap.add_argument("--cpu-iters", type=int, default=60, help="CPU-baseline sample in the phx arm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    import phoenix_b200 as pb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    n = args.n
+    wl = workload(n)
+    sp = system(pb, n, args.dtype, local)
+    solver = pb.Solver(sp)
+    solver.set_field("psi_plus", wl["psi0"])
+    solver.set_field("n_plus", np.zeros((n, n)))
+    solver.set_field("pump_plus", wl["pump"], 0)
+    solver.set_field("potential_plus", wl["potential"], 0)
+    solver.set_field("fft_mask_plus", wl["mask"])
+    stream = torch.cuda.ExternalStream(solver.stream, device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        solver.run(1)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    # timed region: per iteration, flush L2 (untimed) then time the iteration
+    idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    smi_index = idx[local] if len(idx) > local and idx[local].strip().isdigit() else str(local)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches = 0
+    filters = 0
+    solver.profile(True)
+    with ClockSampler(smi_index) as clocks:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[i].record(stream)
+            info = solver.run(1)
+            with torch.cuda.stream(stream):
+                ends[i].record(stream)
+            launches += info.kernel_launches
+            filters += info.fft_filters
+        torch.cuda.synchronize()
+    prof = solver.profile_read()
+    solver.profile(False)
+    step_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+    t_local = torch.tensor([step_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    step_ms = float(t_local.item())
+
+    # back-to-back (L2-warm) iterations, one event pair
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    solver.run(args.steps)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    torch.cuda.synchronize()
+    warm_ms = e0.elapsed_time(e1) / args.steps
+    solver.close()
+
+    # end to end through the public API, host buffers in and out
+    e2e_iters = args.steps
+    chunk = 100
+    pinned_psi = torch.from_numpy(np.ascontiguousarray(wl["psi0"])).pin_memory().numpy()
+    barrier()
+    torch.cuda.synchronize()
+    s2 = pb.Solver(sp)
+    s2.set_field("pump_plus", wl["pump"], 0)
+    s2.set_field("potential_plus", wl["potential"], 0)
+    s2.set_field("fft_mask_plus", wl["mask"])
+    torch.cuda.synchronize()
+    st2 = torch.cuda.ExternalStream(s2.stream, device=local)
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st2):
+        a0.record(st2)
+    s2.set_field("psi_plus", pinned_psi)
+    s2.set_field("n_plus", np.zeros((n, n)))
+    done = 0
+    norms = []
+    while done < e2e_iters:
+        k = min(chunk, e2e_iters - done)
+        s2.run(k)
+        norms.append(s2.sum_abs2("psi_plus"))
+        done += k
+    psi_out = s2.get_field("psi_plus")
+    n_out = s2.get_field("n_plus")
+    with torch.cuda.stream(st2):
+        a1.record(st2)
+    torch.cuda.synchronize()
+    e2e_ms = a0.elapsed_time(a1) / e2e_iters
+    s2.close()
+    t_e2e = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t_e2e.item())
+    esz = 4 if args.dtype == "f32" else 8
+    h2d = n * n * (2 * 8 + 8)  # psi0 (complex) and n0 from FP64 host arrays
+    d2h = n * n * (2 * 8 + 8) + 16 * ((e2e_iters + chunk - 1) // chunk)
+    assert np.isfinite(psi_out).all() and np.isfinite(n_out).all() and all(np.isfinite(norms))
+
+    # roofline of the dominant kernel (fused RK4 middle stage)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_src = "measured"
+    dom = prof.get("rk4_mid", {"ms": float("nan"), "launches": 1, "bytes": float("nan")})
+    per_launch_bytes = dom["bytes"] / dom["launches"]
+    per_launch_ms = dom["ms"] / dom["launches"]
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "rk4_mid_stage_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tj = json.load(f)
+        if tj.get("dtype") == args.dtype and tj.get("n") == n:
+            traffic = tj.get("bytes_per_launch")
+    step_bytes = sum(v["bytes"] for k, v in prof.items() if k.startswith("rk4")) / args.steps
+    kernels_ms = {k: v["ms"] / v["launches"] for k, v in prof.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = reference_cpu_run(n, args.dtype, args.cpu_iters, wl)
+        kind = "reference"
+        if res is None:
+            res = oracle_port_run(n, args.dtype, 3, wl)
+            kind = "port"
+        us, cores, what = res
+        cpu = {"value": us, "unit": "us/iter", "cores": cores, "kind": kind,
+               "sample": f"{args.cpu_iters if kind == 'reference' else 3} RK4 iterations of the {n}^2 workload "
+                         f"with {what}"}
+
+    if rank == 0:
+        us = step_ms * 1e3
+        line = {"metric": METRIC, "value": us, "unit": "us/iter", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": args.dtype, "data": "synthetic", "config": config_dict(args),
+                "grid_point_updates_per_s": world * n * n / (step_ms * 1e-3),
+                "warm_l2_us_per_iter": warm_ms * 1e3,
+                "e2e": {"value": e2e_ms * 1e3, "unit": "us/iter", "h2d_bytes_per_step": h2d / e2e_iters,
+                        "d2h_bytes_per_step": d2h / e2e_iters},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": "stage_scalar_kernel<rk4_mid>",
+                             "peak_source": peak_src, "bytes_per_launch": per_launch_bytes,
+                             "step_alg_bytes": step_bytes,
+                             "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},
+                "kernel_avg_ms": kernels_ms, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
+                "clocks": clocks.summary(), "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

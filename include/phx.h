@@ -33,6 +33,12 @@ extern "C" {
 
 #define PHX_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define PHX_API __attribute__((visibility("default")))
+#else
+#define PHX_API
+#endif
+
 typedef enum {
     PHX_OK = 0,
     PHX_ERR_INVALID_ARG = 1,  /* bad size, pointer, enum or parameter      */
@@ -117,61 +123,85 @@ typedef struct phx_handle phx_handle;
 
 /* Replaces SolverFactory::create + Solver::initialize (solver_factory.hpp:53-60,
  * solver_initialization.cu:13-35): allocate and zero all state for `p`. */
-phx_status phx_create(const phx_params* p, phx_handle** out);
+PHX_API phx_status phx_create(const phx_params* p, phx_handle** out);
 
 /* Frees every device buffer and stream of the handle (no reference
  * counterpart: the reference never frees).  NULL is accepted. */
-phx_status phx_destroy(phx_handle* h);
+PHX_API phx_status phx_destroy(phx_handle* h);
 
 /* Replaces the host->device upload of one matrix
  * (initializeMatricesFromSystem, solver_initialization.cu:37-174, and
  * CUDAMatrix::hostToDeviceSync, cuda_matrix.cuh:281-306).  `host` holds
  * count = N_c*N_r values (complex fields: 2*N_c*N_r reals) of type
  * host_dtype; group selects the temporal group of pump/potential/pulse. */
-phx_status phx_set_field(phx_handle* h, int32_t field, int32_t group, const void* host, int64_t count, int32_t host_dtype);
+PHX_API phx_status phx_set_field(phx_handle* h, int32_t field, int32_t group, const void* host, int64_t count, int32_t host_dtype);
 
 /* Replaces CUDAMatrix::getFullMatrix (device->host, cuda_matrix.cuh:375-403,
  * used by outputMatrices, solver_output_matrices.cu:20-70). */
-phx_status phx_get_field(phx_handle* h, int32_t field, int32_t group, void* host, int64_t count, int32_t host_dtype);
+PHX_API phx_status phx_get_field(phx_handle* h, int32_t field, int32_t group, void* host, int64_t count, int32_t host_dtype);
 
 /* Replaces Envelope::addTemporal (envelope.cpp:88-120) for one group. */
-phx_status phx_set_temporal(phx_handle* h, int32_t envelope, int32_t group, int32_t kind, double t0, double sigma,
+PHX_API phx_status phx_set_temporal(phx_handle* h, int32_t envelope, int32_t group, int32_t kind, double t0, double sigma,
                             double freq);
 
 /* Replaces the main loop's calls of Solver::iterate (main.cu:80-117,
  * solver.cu:22-70): run iterate() until t >= t_max or max_iterations calls. */
-phx_status phx_step(phx_handle* h, int64_t max_iterations, phx_step_info* info);
+PHX_API phx_status phx_step(phx_handle* h, int64_t max_iterations, phx_step_info* info);
 
 /* Current t and dt (SystemParameters::p.t / p.dt). */
-phx_status phx_get_time(phx_handle* h, double* t, double* dt);
+PHX_API phx_status phx_get_time(phx_handle* h, double* t, double* dt);
 
 /* Overwrite t and dt (--t0 / --dt, and the main loop's last-step dt
  * adjustment, main.cu:86-101). */
-phx_status phx_set_time(phx_handle* h, double t, double dt);
+PHX_API phx_status phx_set_time(phx_handle* h, double t, double dt);
 
 /* Sum over grid points of |field|^2 accumulated in FP64 (the reference's
  * transformReduce with transform_abs2, cuda_matrix.cuh:614-632, without
  * halo cells).  Real fields sum their squares. */
-phx_status phx_sum_abs2(phx_handle* h, int32_t field, double* out);
+PHX_API phx_status phx_sum_abs2(phx_handle* h, int32_t field, double* out);
 
 /* Borrow the device pointer of a field for zero-copy interop (e.g. torch):
  * pointer to grid point (0,0), row pitch in elements.  Valid until the
  * handle is destroyed; the caller must order its own work on the handle's
  * stream (phx_get_stream). */
-phx_status phx_field_device_ptr(phx_handle* h, int32_t field, int32_t group, void** dev_ptr, int64_t* row_pitch_elems);
+PHX_API phx_status phx_field_device_ptr(phx_handle* h, int32_t field, int32_t group, void** dev_ptr, int64_t* row_pitch_elems);
+
+/* Kernel families for phx_profile_read */
+typedef enum {
+    PHX_KERNEL_RK4_FIRST = 0,   /* fused RK4 stage 1                         */
+    PHX_KERNEL_RK4_MID = 1,     /* fused RK4 stages 2 and 3                  */
+    PHX_KERNEL_RK4_LAST = 2,    /* fused RK4 stage 4 (in-place update)       */
+    PHX_KERNEL_STAGE = 3,       /* fused k-stack stage (DP45 stages 1-6)     */
+    PHX_KERNEL_STAGE_FINAL = 4, /* fused k-stack final stage (fixed DP45)    */
+    PHX_KERNEL_STAGE_ERROR = 5, /* DP45 k7 + error / norm reduction          */
+    PHX_KERNEL_FILTER = 6,      /* k-space filter passes (without cuFFT)     */
+    PHX_KERNEL_OTHER = 7,       /* rings, reductions                         */
+    PHX_KERNEL_KINDS = 8
+} phx_kernel_kind;
+
+/* Per-launch CUDA-event timing of this handle's kernels (no reference
+ * counterpart: the reference only times its whole loop, misc/timeit.hpp:27-35).
+ * While enabled every launch is bracketed by events on the handle's stream;
+ * enabling resets the totals. */
+PHX_API phx_status phx_profile_enable(phx_handle* h, int32_t enable);
+
+/* Totals since phx_profile_enable(h, 1) for one phx_kernel_kind: device
+ * milliseconds, launches, and the algorithmic bytes those launches must move
+ * to or from HBM (each input and output plane touched once per point). */
+PHX_API phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes);
 
 /* The handle's cudaStream_t, as void*. */
-phx_status phx_get_stream(phx_handle* h, void** stream);
+PHX_API phx_status phx_get_stream(phx_handle* h, void** stream);
 
 /* Message of the last failed call on this handle (or of the last failed
  * phx_create in this thread when h is NULL). */
-const char* phx_last_error(const phx_handle* h);
+PHX_API const char* phx_last_error(const phx_handle* h);
 
-const char* phx_status_string(int32_t status);
+PHX_API const char* phx_status_string(int32_t status);
 
 /* ABI version and build description ("sm_100a ..."). */
-int32_t phx_abi_version(void);
-const char* phx_build_info(void);
+PHX_API int32_t phx_abi_version(void);
+PHX_API const char* phx_build_info(void);
 
 #ifdef __cplusplus
 }

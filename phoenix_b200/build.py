@@ -1,0 +1,58 @@
+"""Build the sm_100a shared library phoenix_b200/libphx.so with nvcc.
+
+The library is built in-tree (not installed) so that it ships with the
+repository to the GPU host.  ``python -m phoenix_b200.build`` rebuilds it;
+``build(force=False)`` skips the compile when the library is newer than
+every source.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "libphx.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
+          "--expt-relaxed-constexpr", "-DPHX_NVCC_VERSION=\"12.9\""]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + \
+        sorted(glob.glob(os.path.join(CSRC, "*.hpp"))) + [os.path.join(ROOT, "include", "phx.h")]
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    cmd = [NVCC] + ARCH_FLAGS + CFLAGS + ["-shared", "-o", LIB + ".tmp", os.path.join(CSRC, "phx_runtime.cu"),
+                                          "-lcufft"]
+    if ptxas_info:
+        cmd.insert(1, "-Xptxas=-v")
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + proc.stdout[-8000:] + proc.stderr[-8000:])
+    if ptxas_info or verbose:
+        sys.stderr.write(proc.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

@@ -86,6 +86,131 @@ __global__ void scatter_interior_kernel(const cx<T>* __restrict__ src, cx<T>* __
     }
 }
 
+// ---- DP45 error norm as the reference takes it over one halo-padded subgrid
+// (halo 7; adaptTimeStep sums rk_error and |buffer_wavefunction_plus|^2 over
+// every padded cell, solver.cu:73-75, cuda_matrix.cuh:614-632,699-705).
+// A padded point at ring distance rho (1..6) holds the stage value written
+// last there, Y_{8-rho} = y0 + stage sum m = 7-rho, and only k_1..k_m were
+// ever computed that far out, so its error term uses e_1..e_m.  Along
+// periodic axes those cells are exact copies of the wrapped interior point;
+// along zero axes they are the computed ring values, stored in place.
+template <typename T>
+struct RingParams {
+    const cx<T>* psi0;  // state (y0)
+    const cx<T>* k;     // k-stack, plane stride
+    long long pitch, plane;
+    int N_r, N_c, periodic_x, periodic_y;
+    T dt;
+    T dtw1;            // dt * a21 (single-weight first stage sum)
+    T a[7][7];         // stage-sum weights, row m-1 builds Y_{m+1}
+    int nw[7];
+    T e[7];            // error weights
+    int passes;        // 1, or 2 where the reference counts the plus error twice
+    double* partials;  // per-block (error, norm)
+};
+
+template <typename T>
+__global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
+    const int B = 6;
+    const long long W = R.N_c + 2LL * B;
+    const long long band_tb = (long long)B * W, band_lr = (long long)R.N_r * B;
+    const long long total = 2 * band_tb + 2 * band_lr;
+    double err = 0.0, nrm = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int r, c;
+        if (t < 2 * band_tb) {
+            const long long u = t % band_tb;
+            r = (t < band_tb ? -B : R.N_r) + (int)(u / W);
+            c = (int)(u % W) - B;
+        } else {
+            const long long u = (t - 2 * band_tb) % band_lr;
+            r = (int)(u / B);
+            c = ((t - 2 * band_tb) < band_lr ? -B : R.N_c) + (int)(u % B);
+        }
+        const int dr = r < 0 ? -r : (r >= R.N_r ? r - R.N_r + 1 : 0);
+        const int dc = c < 0 ? -c : (c >= R.N_c ? c - R.N_c + 1 : 0);
+        const int rho = max(dr, dc);
+        const int sr = (dr && R.periodic_y) ? (r + R.N_r) % R.N_r : r;
+        const int sc = (dc && R.periodic_x) ? (c + R.N_c) % R.N_c : c;
+        const long long idx = (long long)sr * R.pitch + sc;
+        const int m = 7 - rho;
+        cx<T> e = mk((T)0, (T)0);
+        for (int j = 0; j < m; ++j) {
+            if (R.e[j] == (T)0) continue;
+            e = cadd(e, smul(R.e[j], R.k[(long long)j * R.plane + idx]));
+        }
+        err += (double)abs2(smul(R.dt, e)) * (double)R.passes;
+        const cx<T> y0 = R.psi0[idx];
+        cx<T> y;
+        if (m == 1) {
+            y = cadd(y0, smul(R.dtw1, R.k[idx]));
+        } else {
+            cx<T> acc = smul(R.a[m - 1][0], R.k[idx]);
+            for (int q = 1; q < R.nw[m - 1]; ++q) acc = cadd(acc, smul(R.a[m - 1][q], R.k[(long long)q * R.plane + idx]));
+            y = cadd(y0, smul(R.dt, acc));
+        }
+        nrm += (double)abs2(y);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        err += __shfl_down_sync(0xffffffffu, err, o);
+        nrm += __shfl_down_sync(0xffffffffu, nrm, o);
+    }
+    __shared__ double s[64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s[2 * warp] = err;
+        s[2 * warp + 1] = nrm;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) {
+            a += s[2 * w];
+            b += s[2 * w + 1];
+        }
+        R.partials[2 * blockIdx.x] = a;
+        R.partials[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// Outer ring (rho == 7) of the state's synchronised halo: images along
+// periodic axes, zero outside any zero axis.  The reference's buffer keeps
+// this ring from the state of the previous accepted step (buffers swap on
+// accept, solver.cu:107-114), so the host carries the value one step.
+template <typename T>
+__global__ void ring7_kernel(const cx<T>* __restrict__ psi0, long long pitch, int N_r, int N_c, int periodic_x,
+                             int periodic_y, double* __restrict__ out) {
+    const int B = 7;
+    const long long W = N_c + 2LL * B;
+    const long long total = 2 * W + 2LL * (N_r + 2 * (B - 1));
+    double a = 0.0;
+    for (long long t = threadIdx.x; t < total; t += blockDim.x) {
+        int r, c;
+        if (t < 2 * W) {
+            r = t < W ? -B : N_r + B - 1;
+            c = (int)(t % W) - B;
+        } else {
+            const long long u = (t - 2 * W) % (N_r + 2LL * (B - 1));
+            r = (int)u - (B - 1);
+            c = (t - 2 * W) < (N_r + 2LL * (B - 1)) ? -B : N_c + B - 1;
+        }
+        const bool out_r = r < 0 || r >= N_r, out_c = c < 0 || c >= N_c;
+        if ((out_r && !periodic_y) || (out_c && !periodic_x)) continue;
+        const int sr = out_r ? (r + N_r) % N_r : r, sc = out_c ? (c + N_c) % N_c : c;
+        a += (double)abs2(psi0[(long long)sr * pitch + sc]);
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    __shared__ double s[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s[warp] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) v += s[w];
+        *out = v;
+    }
+}
+
 // Sum of n (error, norm) pairs in a fixed order: one block, deterministic.
 __global__ void finalize_pairs_kernel(const double* __restrict__ partials, long long n, double* __restrict__ out) {
     __shared__ double sa[32], sb[32];

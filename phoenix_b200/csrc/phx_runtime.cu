@@ -1,0 +1,1044 @@
+// phx_runtime.cu -- the handle behind include/phx.h.
+//
+// Owns the device state of one simulation (halo-padded planes, see
+// phx_device.cuh), runs the iteration loop of Solver::iterate
+// (source/cuda_solver/solver/solver.cu:22-70) with t, dt and every host-side
+// scalar kept in the build precision, launches one fused kernel per RK stage
+// (phx_stage.cuh), performs DP45 step-size control with FP64 reductions
+// (Solver::adaptTimeStep, solver.cu:72-105) and applies the k-space mask
+// filter through cuFFT (Solver::applyFFTFilter, solver_fft.cu:67-119).
+#include <cufft.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <functional>
+#include <limits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/phx.h"
+#include "phx_host.hpp"
+#include "phx_misc.cuh"
+#include "phx_stage.cuh"
+#include "phx_stage_tetm.cuh"
+
+namespace phx {
+
+thread_local std::string g_create_error;
+
+struct Error {
+    phx_status status;
+    std::string msg;
+};
+
+#define PHX_CUDA(call)                                                                                       \
+    do {                                                                                                     \
+        cudaError_t e_ = (call);                                                                             \
+        if (e_ != cudaSuccess) throw Error{PHX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+#define PHX_CUFFT(call)                                                                       \
+    do {                                                                                      \
+        cufftResult r_ = (call);                                                              \
+        if (r_ != CUFFT_SUCCESS) throw Error{PHX_ERR_CUDA, std::string(#call) + " failed (" + \
+                                             std::to_string((int)r_) + ")"};                  \
+    } while (0)
+
+static void fail(phx_status s, const std::string& m) { throw Error{s, m}; }
+
+// ---------------------------------------------------------------- device memory
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    void alloc(size_t n, cudaStream_t s) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = n;
+        if (n == 0) return;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            (void)cudaGetLastError();
+            fail(PHX_ERR_OOM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
+        }
+        PHX_CUDA(cudaMemsetAsync(p, 0, n, s));
+    }
+};
+
+struct PinnedBuf {
+    void* p = nullptr;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void alloc(size_t n) {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        PHX_CUDA(cudaMallocHost(&p, n));
+    }
+};
+
+// ---------------------------------------------------------------- engine
+struct EngineBase {
+    phx_params P{};
+    cudaStream_t stream = nullptr;
+    int64_t launches = 0;
+    std::string last_error;
+    TemporalSpec pump_t[kMaxGroups], pot_t[kMaxGroups], pulse_t[kMaxGroups];
+    virtual ~EngineBase() = default;
+    virtual void init() = 0;
+    virtual void set_field(int field, int group, const void* host, int64_t count, int dtype) = 0;
+    virtual void get_field(int field, int group, void* host, int64_t count, int dtype) = 0;
+    virtual void step(int64_t max_iterations, phx_step_info* info) = 0;
+    virtual void get_time(double* t, double* dt) = 0;
+    virtual void set_time(double t, double dt) = 0;
+    virtual double sum_abs2(int field) = 0;
+    virtual void field_ptr(int field, int group, void** ptr, int64_t* pitch) = 0;
+
+    // ---- per-launch event timing (phx_profile_*)
+    bool profiling = false;
+    struct Pending {
+        int kind;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double prof_ms[PHX_KERNEL_KINDS] = {};
+    double prof_bytes[PHX_KERNEL_KINDS] = {};
+    int64_t prof_count[PHX_KERNEL_KINDS] = {};
+    cudaEvent_t get_event() {
+        if (!event_pool.empty()) {
+            cudaEvent_t e = event_pool.back();
+            event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        PHX_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    void prof_begin(cudaEvent_t& a) {
+        if (!profiling) return;
+        a = get_event();
+        PHX_CUDA(cudaEventRecord(a, stream));
+    }
+    void prof_end(int kind, cudaEvent_t a, double bytes) {
+        if (!profiling) return;
+        cudaEvent_t b = get_event();
+        PHX_CUDA(cudaEventRecord(b, stream));
+        pending.push_back({kind, a, b, bytes});
+    }
+    void prof_harvest() {
+        if (pending.empty()) return;
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        for (auto& p : pending) {
+            float ms = 0.f;
+            PHX_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+            prof_ms[p.kind] += ms;
+            prof_bytes[p.kind] += p.bytes;
+            prof_count[p.kind] += 1;
+            event_pool.push_back(p.a);
+            event_pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void prof_reset() {
+        prof_harvest();
+        for (int k = 0; k < PHX_KERNEL_KINDS; ++k) prof_ms[k] = prof_bytes[k] = 0, prof_count[k] = 0;
+    }
+};
+
+template <typename T>
+struct Engine final : EngineBase {
+    static constexpr int G = kRing;
+    static constexpr int CPT = Pack<T>::CPT;
+    static constexpr int RB = 8;
+    static constexpr int kRingBlocks = 64;
+    using C = cx<T>;
+
+    int N_r = 0, N_c = 0;
+    long long pitch = 0, rows = 0, plane = 0;
+    Derived<T> d{};
+    int comps = 1;
+    int H = 4;  // halo width the reference uses: k_max of the iterator
+
+    // state and work planes (each allocation holds 1 or more planes)
+    DevBuf psi[2], nres[2];            // state per component
+    DevBuf sbuf_psi[2][2], sbuf_n[2][2];  // [component][ping-pong] stage values
+    DevBuf acc_psi[2], acc_n[2];       // RK4 accumulators
+    DevBuf k_psi[2], k_n[2];           // DP45 k-stack (7 planes)
+    DevBuf pump[2], pot[2], pulse[2];  // input planes (groups)
+    DevBuf mask[2];                    // fft-shifted mask, contiguous N_r*N_c
+    DevBuf fft_x;                      // contiguous scratch for the filter
+    DevBuf partials, result;
+    PinnedBuf host_result;
+    cufftHandle plan = 0;
+    bool have_plan = false;
+    bool have_mask[2] = {false, false};
+
+    // simulation clock, in the build precision (SystemParameters::p.t / p.dt)
+    T t = 0, dt = 0, fft_cached_t = 0;
+    double r7_prev = 0, r7_cur = 0;  // DP45 reference norm: outer halo ring carried between steps
+    int64_t accepted_steps = 0;
+
+    ~Engine() override {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& p : pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        for (auto e : event_pool) cudaEventDestroy(e);
+        if (have_plan) cufftDestroy(plan);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    C* cplane(DevBuf& b, int k = 0) { return reinterpret_cast<C*>(b.p) + G * pitch + G + (long long)k * plane; }
+    T* rplane(DevBuf& b, int k = 0) { return reinterpret_cast<T*>(b.p) + G * pitch + G + (long long)k * plane; }
+
+    void init() override {
+        N_r = P.N_r;
+        N_c = P.N_c;
+        comps = P.tetm ? 2 : 1;
+        H = P.iterator == PHX_ITER_DP45 ? 7 : 4;
+        pitch = ((N_c + 2LL * G) + 31) / 32 * 32;
+        rows = N_r + 2LL * G;
+        plane = pitch * rows;
+        d = derive<T>(P);
+        PHX_CUDA(cudaSetDevice(P.device));
+        PHX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        const size_t cb = sizeof(C) * plane, rb = sizeof(T) * plane;
+        for (int q = 0; q < comps; ++q) {
+            psi[q].alloc(cb, stream);
+            nres[q].alloc(rb, stream);
+            for (int b = 0; b < 2; ++b) {
+                sbuf_psi[q][b].alloc(cb, stream);
+                sbuf_n[q][b].alloc(rb, stream);
+            }
+            if (P.iterator == PHX_ITER_RK4) {
+                acc_psi[q].alloc(cb, stream);
+                acc_n[q].alloc(rb, stream);
+            } else {
+                k_psi[q].alloc(cb * 7, stream);
+                k_n[q].alloc(rb * 7, stream);
+            }
+            pump[q].alloc(rb * std::max(1, P.n_pump_groups), stream);
+            pot[q].alloc(rb * std::max(1, P.n_potential_groups), stream);
+            pulse[q].alloc(cb * std::max(1, P.n_pulse_groups), stream);
+        }
+        const long long max_blocks = grid_x(-(long long)G, N_c + G) * grid_y(-(long long)G, N_r + G) + 64;
+        partials.alloc(sizeof(double) * 2 * std::max<long long>(max_blocks, 1024), stream);
+        result.alloc(sizeof(double) * 4, stream);
+        host_result.alloc(sizeof(double) * 4);
+        t = (T)P.t0;
+        dt = (T)P.dt;
+        fft_cached_t = (T)0.0;
+        PHX_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
+    long long grid_y(long long r0, long long r1) const { return (r1 - r0 + kStageWarps * RB - 1) / (kStageWarps * RB); }
+
+    // ------------------------------------------------------------ fields
+    struct FieldRef {
+        DevBuf* buf;
+        bool complex;
+        int plane_index;
+        int comp;
+    };
+    FieldRef field_ref(int field, int group) {
+        const int comp = (field == PHX_PSI_MINUS || field == PHX_N_MINUS || field == PHX_PUMP_MINUS ||
+                          field == PHX_POTENTIAL_MINUS || field == PHX_PULSE_MINUS || field == PHX_FFT_MASK_MINUS)
+                             ? 1
+                             : 0;
+        if (comp == 1 && !P.tetm) fail(PHX_ERR_INVALID_ARG, "minus-component field requires tetm mode");
+        switch (field) {
+            case PHX_PSI_PLUS:
+            case PHX_PSI_MINUS:
+                return {&psi[comp], true, 0, comp};
+            case PHX_N_PLUS:
+            case PHX_N_MINUS:
+                if (!P.use_reservoir) fail(PHX_ERR_INVALID_ARG, "reservoir field requires use_reservoir");
+                return {&nres[comp], false, 0, comp};
+            case PHX_PUMP_PLUS:
+            case PHX_PUMP_MINUS:
+                if (group < 0 || group >= P.n_pump_groups) fail(PHX_ERR_INVALID_ARG, "pump group out of range");
+                return {&pump[comp], false, group, comp};
+            case PHX_POTENTIAL_PLUS:
+            case PHX_POTENTIAL_MINUS:
+                if (group < 0 || group >= P.n_potential_groups) fail(PHX_ERR_INVALID_ARG, "potential group out of range");
+                return {&pot[comp], false, group, comp};
+            case PHX_PULSE_PLUS:
+            case PHX_PULSE_MINUS:
+                if (group < 0 || group >= P.n_pulse_groups) fail(PHX_ERR_INVALID_ARG, "pulse group out of range");
+                return {&pulse[comp], true, group, comp};
+            default:
+                fail(PHX_ERR_INVALID_ARG, "unknown field " + std::to_string(field));
+        }
+        return {nullptr, false, 0, 0};
+    }
+
+    static void convert_in(const void* host, int dtype, size_t n, std::vector<T>& out) {
+        out.resize(n);
+        if (dtype == PHX_F64) {
+            const double* s = static_cast<const double*>(host);
+            for (size_t i = 0; i < n; ++i) out[i] = (T)s[i];
+        } else {
+            const float* s = static_cast<const float*>(host);
+            for (size_t i = 0; i < n; ++i) out[i] = (T)s[i];
+        }
+    }
+
+    void set_field(int field, int group, const void* host, int64_t count, int dtype) override {
+        if (!host) fail(PHX_ERR_INVALID_ARG, "host pointer is NULL");
+        if (dtype != PHX_F32 && dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "bad host dtype");
+        const long long N = (long long)N_r * N_c;
+        if (field == PHX_FFT_MASK_PLUS || field == PHX_FFT_MASK_MINUS) {
+            const int comp = field == PHX_FFT_MASK_MINUS ? 1 : 0;
+            if (comp == 1 && !P.tetm) fail(PHX_ERR_INVALID_ARG, "minus mask requires tetm");
+            if (count != N) fail(PHX_ERR_INVALID_ARG, "mask needs N_c*N_r values");
+            std::vector<T> m;
+            convert_in(host, dtype, (size_t)N, m);
+            // fft_shift_2D (kernel_fft.cuh:16-32), done once on the host
+            for (int k = 0; k < N_r / 2; ++k)
+                for (int l = 0; l < N_c / 2; ++l) {
+                    std::swap(m[(size_t)k * N_c + l], m[(size_t)(k + N_r / 2) * N_c + l + N_c / 2]);
+                    std::swap(m[(size_t)k * N_c + l + N_c / 2], m[(size_t)(k + N_r / 2) * N_c + l]);
+                }
+            if (!mask[comp].p) mask[comp].alloc(sizeof(T) * N, stream);
+            PHX_CUDA(cudaMemcpyAsync(mask[comp].p, m.data(), sizeof(T) * N, cudaMemcpyHostToDevice, stream));
+            PHX_CUDA(cudaStreamSynchronize(stream));
+            have_mask[comp] = true;
+            ensure_fft();
+            return;
+        }
+        FieldRef f = field_ref(field, group);
+        const long long want = f.complex ? 2 * N : N;
+        if (count != want) fail(PHX_ERR_INVALID_ARG, "expected " + std::to_string(want) + " values, got " + std::to_string(count));
+        std::vector<T> tmp;
+        convert_in(host, dtype, (size_t)want, tmp);
+        const size_t esz = f.complex ? sizeof(C) : sizeof(T);
+        char* dst = reinterpret_cast<char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
+        PHX_CUDA(cudaMemcpy2DAsync(dst, esz * pitch, tmp.data(), esz * N_c, esz * N_c, N_r, cudaMemcpyHostToDevice, stream));
+        if (field == PHX_PSI_PLUS || field == PHX_PSI_MINUS) {
+            ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(*f.buf), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
+            PHX_CUDA(cudaGetLastError());
+        }
+        PHX_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void get_field(int field, int group, void* host, int64_t count, int dtype) override {
+        if (!host) fail(PHX_ERR_INVALID_ARG, "host pointer is NULL");
+        if (dtype != PHX_F32 && dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "bad host dtype");
+        if (field == PHX_FFT_MASK_PLUS || field == PHX_FFT_MASK_MINUS) fail(PHX_ERR_UNSUPPORTED, "mask read-back not provided");
+        FieldRef f = field_ref(field, group);
+        const long long N = (long long)N_r * N_c;
+        const long long want = f.complex ? 2 * N : N;
+        if (count != want) fail(PHX_ERR_INVALID_ARG, "expected " + std::to_string(want) + " values");
+        std::vector<T> tmp((size_t)want);
+        const size_t esz = f.complex ? sizeof(C) : sizeof(T);
+        const char* src = reinterpret_cast<const char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
+        PHX_CUDA(cudaMemcpy2DAsync(tmp.data(), esz * N_c, src, esz * pitch, esz * N_c, N_r, cudaMemcpyDeviceToHost, stream));
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        if (dtype == PHX_F64) {
+            double* o = static_cast<double*>(host);
+            for (long long i = 0; i < want; ++i) o[i] = (double)tmp[i];
+        } else {
+            float* o = static_cast<float*>(host);
+            for (long long i = 0; i < want; ++i) o[i] = (float)tmp[i];
+        }
+    }
+
+    void field_ptr(int field, int group, void** ptr, int64_t* pp) override {
+        FieldRef f = field_ref(field, group);
+        const size_t esz = f.complex ? sizeof(C) : sizeof(T);
+        *ptr = reinterpret_cast<char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
+        if (pp) *pp = pitch;
+    }
+
+    void ensure_fft() {
+        if (have_plan) return;
+        fft_x.alloc(sizeof(C) * (size_t)N_r * N_c, stream);
+        // the reference plans (N_c, N_r) on the full N_r x N_c matrix (solver_fft.cu:35-48)
+        PHX_CUFFT(cufftPlan2d(&plan, N_c, N_r, sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z));
+        PHX_CUFFT(cufftSetStream(plan, stream));
+        have_plan = true;
+    }
+
+    void get_time(double* tt, double* dd) override {
+        if (tt) *tt = (double)t;
+        if (dd) *dd = (double)dt;
+    }
+    void set_time(double tt, double dd) override {
+        t = (T)tt;
+        dt = (T)dd;
+    }
+
+    // ------------------------------------------------------------ stage launch
+    StageParams<T> base_params(int comp) {
+        StageParams<T> S;
+        std::memset(&S, 0, sizeof(S));
+        S.N_r = N_r;
+        S.N_c = N_c;
+        S.img_x = P.periodic_x;
+        S.img_y = P.periodic_y;
+        S.pitch = pitch;
+        S.plane = plane;
+        S.m2 = d.m2;
+        S.odx2 = d.odx2;
+        S.ody2 = d.ody2;
+        S.meff = d.meff;
+        S.ohb = d.ohb;
+        S.ohb_gc = d.ohb * (T)P.g_c;
+        S.half_gamma_c = (T)0.5 * (T)P.gamma_c;
+        S.ohb_gr = d.ohb * (T)P.g_r;
+        S.half_R = (T)0.5 * (T)P.R;
+        S.gamma_r = (T)P.gamma_r;
+        S.R = (T)P.R;
+        (void)comp;
+        S.n_pump = P.n_pump_groups;
+        S.n_pot = P.n_potential_groups;
+        S.n_pulse = P.n_pulse_groups;
+        S.dt = dt;
+        S.error_passes = 1;
+        return S;
+    }
+
+    // temporal amplitudes at t (amp) and t+dt (amp_next): updateKernelTime
+    std::complex<T> amp_pump[kMaxGroups], next_pump[kMaxGroups];
+    std::complex<T> amp_pot[kMaxGroups], next_pot[kMaxGroups];
+    std::complex<T> amp_pulse[kMaxGroups], next_pulse[kMaxGroups];
+    void update_kernel_time() {
+        const T tn = t + dt;
+        for (int g = 0; g < P.n_pulse_groups; ++g) amp_pulse[g] = temporal_value<T>(pulse_t[g], t);
+        for (int g = 0; g < P.n_potential_groups; ++g) amp_pot[g] = temporal_value<T>(pot_t[g], t);
+        for (int g = 0; g < P.n_pump_groups; ++g) amp_pump[g] = temporal_value<T>(pump_t[g], t);
+        for (int g = 0; g < P.n_pulse_groups; ++g) next_pulse[g] = temporal_value<T>(pulse_t[g], tn);
+        for (int g = 0; g < P.n_potential_groups; ++g) next_pot[g] = temporal_value<T>(pot_t[g], tn);
+        for (int g = 0; g < P.n_pump_groups; ++g) {
+            next_pump[g] = temporal_value<T>(pump_t[g], tn);
+            if (amp_pump[g].imag() != (T)0 || next_pump[g].imag() != (T)0)
+                fail(PHX_ERR_UNSUPPORTED, "complex pump temporal envelopes (iexp) would make the reservoir complex");
+        }
+    }
+    void set_coefficients(StageParams<T>& S, T w) {
+        for (int g = 0; g < P.n_pump_groups; ++g) {
+            const auto c = interp<T>(amp_pump[g], next_pump[g], w);
+            S.pump_c[g] = mk_host(c);
+        }
+        for (int g = 0; g < P.n_potential_groups; ++g) S.pot_c[g] = mk_host(interp<T>(amp_pot[g], next_pot[g], w));
+        for (int g = 0; g < P.n_pulse_groups; ++g) S.pulse_c[g] = mk_host(interp<T>(amp_pulse[g], next_pulse[g], w));
+    }
+    static C mk_host(std::complex<T> z) {
+        C c;
+        c.re = z.real();
+        c.im = z.imag();
+        return c;
+    }
+
+    // compute rectangle of stage s (1-based) of an H-stage step: the subgrid
+    // extended by H - s cells along non-periodic axes (cuda_macro.cuh:110-113)
+    void region(StageParams<T>& S, int ext) {
+        const int ex = P.periodic_x ? 0 : ext;
+        const int ey = P.periodic_y ? 0 : ext;
+        S.r0 = -ey;
+        S.r1 = N_r + ey;
+        int c0 = -ex, c1 = N_c + ex;
+        c0 = (c0 >= 0) ? (c0 / CPT) * CPT : -((-c0 + CPT - 1) / CPT) * CPT;
+        c1 = ((c1 + CPT - 1) / CPT) * CPT;
+        S.c0 = c0;
+        S.c1 = c1;
+    }
+
+    // Algorithmic HBM bytes of one stage launch: every plane the kernel
+    // reads or writes, once per point of its rectangle.
+    double stage_bytes(int KIND, bool RES, const StageParams<T>& S) const {
+        const double c = sizeof(C), r = sizeof(T);
+        const double st = c + (RES ? r : 0.0);  // one state (psi, n)
+        const double inputs = S.n_pump * r + S.n_pot * r + S.n_pulse * c;
+        double b = 0;
+        switch (KIND) {
+            case kRk4First: b = st + inputs + 2 * st; break;
+            case kRk4Mid: b = 3 * st + inputs + 2 * st; break;
+            case kRk4Last: b = 3 * st + inputs + st; break;
+            case kStack: {
+                const int kreads = S.nw > 1 ? S.nw - 1 : 0;
+                b = st + (S.stage > 1 ? st : 0) + kreads * st + inputs + 2 * st;
+                break;
+            }
+            case kStackFinal: b = 2 * st + (S.nw - 1) * st + inputs + st; break;
+            case kStackError: b = st + (S.nw - 1) * c + inputs; break;
+        }
+        return b * (double)(S.r1 - S.r0) * (double)(S.c1 - S.c0);
+    }
+    template <int KIND, bool RES>
+    void launch_kind(const StageParams<T>& S) {
+        dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        stage_scalar_kernel<T, KIND, RES, RB><<<grid, 32 * kStageWarps, 0, stream>>>(S);
+        prof_end(KIND, a, stage_bytes(KIND, RES, S));
+        ++launches;
+    }
+    // Launch stage KIND.  `wire(S, q)` points S at component q's planes; in
+    // TE/TM mode the minus component's planes are wired the same way and
+    // both polarisations run in one kernel.
+    template <int KIND, typename Wire>
+    void launch(StageParams<T>& S, Wire wire) {
+        wire(S, 0);
+        if (P.tetm) {
+            TetmParams<T> Q;
+            std::memset(&Q, 0, sizeof(Q));
+            Q.p = S;
+            StageParams<T> M = S;
+            wire(M, 1);
+            Q.psi_in = M.psi_in, Q.n_in = M.n_in, Q.psi0 = M.psi0, Q.n0 = M.n0, Q.psi_out = M.psi_out;
+            Q.n_out = M.n_out, Q.acc_psi = M.acc_psi, Q.acc_n = M.acc_n, Q.k_psi = M.k_psi, Q.k_n = M.k_n;
+            Q.pump = M.pump, Q.pot = M.pot, Q.pulse = M.pulse;
+            Q.ohb_meff = d.ohb * d.meff;
+            Q.ohb_gpm = d.ohb * (T)P.g_pm;
+            Q.ohb_dlt = d.ohb * (T)P.delta_LT;
+            Q.hidd.re = (T)0.0 / d.dx / d.dy;
+            Q.hidd.im = (T)0.5 / d.dx / d.dy;
+            dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
+            cudaEvent_t a = nullptr;
+            prof_begin(a);
+            stage_tetm_kernel<T, KIND, RB><<<grid, 32 * kStageWarps, 0, stream>>>(Q);
+            prof_end(KIND, a, 2 * stage_bytes(KIND, true, S));
+            ++launches;
+        } else if (P.use_reservoir) {
+            launch_kind<KIND, true>(S);
+        } else {
+            launch_kind<KIND, false>(S);
+        }
+        PHX_CUDA(cudaGetLastError());
+    }
+
+    // ------------------------------------------------------------ RK4
+    void step_rk4() {
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
+        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
+        for (int s = 1; s <= 4; ++s) {
+            StageParams<T> S = base_params(0);
+            set_coefficients(S, cw[s - 1]);
+            region(S, 4 - s);
+            S.stage = s;
+            S.b = bw[s - 1];
+            if (s < 4) S.dtw = dt * aw[s - 1];
+            auto wire = [this, s](StageParams<T>& X, int q) {
+                X.psi0 = cplane(psi[q]);
+                X.n0 = rplane(nres[q]);
+                X.psi_in = s == 1 ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 2) & 1]);
+                X.n_in = s == 1 ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 2) & 1]);
+                X.psi_out = s == 4 ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 1) & 1]);
+                X.n_out = s == 4 ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 1) & 1]);
+                X.acc_psi = cplane(acc_psi[q]);
+                X.acc_n = rplane(acc_n[q]);
+                X.pump = rplane(pump[q]);
+                X.pot = rplane(pot[q]);
+                X.pulse = cplane(pulse[q]);
+            };
+            if (s == 1)
+                launch<kRk4First>(S, wire);
+            else if (s < 4)
+                launch<kRk4Mid>(S, wire);
+            else
+                launch<kRk4Last>(S, wire);
+        }
+    }
+
+    // ------------------------------------------------------------ DP45
+    // Butcher tableau of DormandPrince45 (dormand_prince.cu:18-35,37-95) in the
+    // operand order of its INTERMEDIATE_SUM_K / ERROR_K calls.
+    static void dp45_rows(T a[7][7], int nw[7], T c[7], T e[7]) {
+        std::memset(a, 0, sizeof(T) * 49);
+        a[0][0] = (T)(1.0 / 5.0);
+        nw[0] = 1;
+        a[1][0] = (T)(3.0 / 40.0), a[1][1] = (T)(9.0 / 40.0);
+        nw[1] = 2;
+        a[2][0] = (T)(44.0 / 45.0), a[2][1] = (T)(-56.0 / 15.0), a[2][2] = (T)(32.0 / 9.0);
+        nw[2] = 3;
+        a[3][0] = (T)(19372.0 / 6561.0), a[3][1] = (T)(-25360.0 / 2187.0), a[3][2] = (T)(64448.0 / 6561.0),
+        a[3][3] = (T)(-212.0 / 729.0);
+        nw[3] = 4;
+        a[4][0] = (T)(9017.0 / 3168.0), a[4][1] = (T)(-355.0 / 33.0), a[4][2] = (T)(46732.0 / 5247.0),
+        a[4][3] = (T)(49.0 / 176.0), a[4][4] = (T)(-5103.0 / 18656.0);
+        nw[4] = 5;
+        a[5][0] = (T)(35.0 / 384.0), a[5][1] = (T)(0.0), a[5][2] = (T)(500.0 / 1113.0), a[5][3] = (T)(125.0 / 192.0),
+        a[5][4] = (T)(-2187.0 / 6784.0), a[5][5] = (T)(11.0 / 84.0);
+        nw[5] = 6;
+        nw[6] = 7;
+        c[0] = (T)0.0, c[1] = (T)(1.0 / 5.0), c[2] = (T)(3.0 / 10.0), c[3] = (T)(4.0 / 5.0), c[4] = (T)(8.0 / 9.0),
+        c[5] = (T)1.0, c[6] = (T)1.0;
+        e[0] = (T)(35.0 / 384.0 - 5179.0 / 57600.0);
+        e[1] = (T)(0.0);
+        e[2] = (T)(500.0 / 1113.0 - 7571.0 / 16695.0);
+        e[3] = (T)(125.0 / 192.0 - 393.0 / 640.0);
+        e[4] = (T)(-2187.0 / 6784.0 + 92097.0 / 339200.0);
+        e[5] = (T)(11.0 / 84.0 - 187.0 / 2100.0);
+        e[6] = (T)(-1.0 / 40.0);
+    }
+
+    long long dp45_stages(bool adaptive, bool ref_norm = false) {
+        T a[7][7], c[7], e[7];
+        int nw[7];
+        dp45_rows(a, nw, c, e);
+        for (int s = 1; s <= 6; ++s) {
+            StageParams<T> S = base_params(0);
+            set_coefficients(S, c[s - 1]);
+            const bool final_fixed = !adaptive && s == 6;
+            region(S, final_fixed ? 0 : 7 - s);
+            S.stage = s;
+            S.nw = nw[s - 1];
+            for (int q = 0; q < S.nw; ++q) S.w[q] = a[s - 1][q];
+            if (S.nw == 1) S.dtw = dt * a[s - 1][0];
+            auto wire = [this, s, final_fixed](StageParams<T>& X, int q) {
+                X.psi0 = cplane(psi[q]);
+                X.n0 = rplane(nres[q]);
+                X.psi_in = s == 1 ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 2) & 1]);
+                X.n_in = s == 1 ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 2) & 1]);
+                X.k_psi = cplane(k_psi[q]);
+                X.k_n = rplane(k_n[q]);
+                X.psi_out = final_fixed ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 1) & 1]);
+                X.n_out = final_fixed ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 1) & 1]);
+                X.pump = rplane(pump[q]);
+                X.pot = rplane(pot[q]);
+                X.pulse = cplane(pulse[q]);
+            };
+            if (final_fixed)
+                launch<kStackFinal>(S, wire);
+            else
+                launch<kStack>(S, wire);
+        }
+        if (!adaptive) return 0;
+        // k7 = f(y6) and the error / norm reduction over the interior
+        StageParams<T> S = base_params(0);
+        set_coefficients(S, c[6]);
+        region(S, 0);
+        S.stage = 7;
+        S.nw = 7;
+        for (int q = 0; q < 7; ++q) S.w[q] = e[q];
+        S.partials = reinterpret_cast<double*>(partials.p);
+        S.error_passes = P.tetm ? 2 : 1;
+        launch<kStackError>(S, [this](StageParams<T>& X, int q) {
+            X.psi0 = cplane(psi[q]);
+            X.n0 = rplane(nres[q]);
+            X.psi_in = cplane(sbuf_psi[q][1]);
+            X.n_in = rplane(sbuf_n[q][1]);
+            X.k_psi = cplane(k_psi[q]);
+            X.k_n = rplane(k_n[q]);
+            X.pump = rplane(pump[q]);
+            X.pot = rplane(pot[q]);
+            X.pulse = cplane(pulse[q]);
+        });
+        long long nb = grid_x(S.c0, S.c1) * grid_y(S.r0, S.r1);
+        if (ref_norm) {
+            RingParams<T> R;
+            std::memset(&R, 0, sizeof(R));
+            R.psi0 = cplane(psi[0]);
+            R.k = cplane(k_psi[0]);
+            R.pitch = pitch;
+            R.plane = plane;
+            R.N_r = N_r;
+            R.N_c = N_c;
+            R.periodic_x = P.periodic_x;
+            R.periodic_y = P.periodic_y;
+            R.dt = dt;
+            R.dtw1 = dt * a[0][0];
+            std::memcpy(R.a, a, sizeof(R.a));
+            std::memcpy(R.nw, nw, sizeof(R.nw));
+            std::memcpy(R.e, e, sizeof(R.e));
+            R.passes = P.tetm ? 2 : 1;
+            R.partials = reinterpret_cast<double*>(partials.p) + 2 * nb;
+            dp45_ring_kernel<T><<<kRingBlocks, 256, 0, stream>>>(R);
+            ++launches;
+            PHX_CUDA(cudaGetLastError());
+            nb += kRingBlocks;
+        }
+        return nb;
+    }
+
+    bool adapt_time_step(double err_sum, double norm_sum) {
+        // Solver::adaptTimeStep with power 1/4 (solver.cu:72-105)
+        const T normalization_factor = (T)norm_sum;
+        const T integrated_error = (T)err_sum;
+        T final_error = std::abs(integrated_error / normalization_factor);
+        const T tol = (T)P.tol;
+        const T lo = std::numeric_limits<T>::min();
+        const T dh_arg = (T)((double)tol / 2.0 / (double)(final_error > lo ? final_error : lo));
+        T dh = (T)std::pow((double)dh_arg, (double)(T)0.25);
+        if (std::isnan(dh)) {
+            dh = (T)0.9;
+            final_error = std::numeric_limits<T>::max();
+        }
+        if (std::isnan(final_error)) {
+            dh = (T)0.9;
+            final_error = std::numeric_limits<T>::max();
+        }
+        const T cand = dt * dh;
+        T new_dt = std::min(cand, (T)P.dt_max);
+        if (new_dt < (T)P.dt_min) new_dt = (T)P.dt_min;
+        dt = new_dt;
+        update_kernel_time();
+        return final_error < tol;
+    }
+
+    void swap_state_with_y6() {
+        for (int q = 0; q < comps; ++q) {
+            std::swap(psi[q].p, sbuf_psi[q][1].p);
+            std::swap(nres[q].p, sbuf_n[q][1].p);
+            if (!(P.periodic_x && P.periodic_y)) {
+                ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(psi[q]), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
+                ring_fill_kernel<T><<<64, 256, 0, stream>>>(rplane(nres[q]), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
+                launches += 2;
+                PHX_CUDA(cudaGetLastError());
+            }
+        }
+    }
+
+    void step_dp45(bool adaptive, int64_t& acc, int64_t& rej) {
+        if (!adaptive) {
+            dp45_stages(false);
+            return;
+        }
+        const bool ref_norm = P.norm_mode == PHX_NORM_REFERENCE;
+        if (ref_norm) {
+            // outer ring of the state's halo at the start of this step -> result[2]
+            ring7_kernel<T><<<1, 1024, 0, stream>>>(cplane(psi[0]), pitch, N_r, N_c, P.periodic_x, P.periodic_y,
+                                                    reinterpret_cast<double*>(result.p) + 2);
+            ++launches;
+            PHX_CUDA(cudaGetLastError());
+        }
+        bool accept = false;
+        do {
+            const long long nb = dp45_stages(true, ref_norm);
+            finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), nb,
+                                                          reinterpret_cast<double*>(result.p));
+            ++launches;
+            PHX_CUDA(cudaGetLastError());
+            PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            PHX_CUDA(cudaStreamSynchronize(stream));
+            const double* r = static_cast<const double*>(host_result.p);
+            double err = r[0], nrm = r[1];
+            if (ref_norm) {
+                // the reference's buffer still holds, in its outermost halo ring,
+                // the state of the previous accepted step (zero before the first)
+                nrm += r7_prev;
+                r7_cur = r[2];
+            }
+            accept = adapt_time_step(err, nrm);
+            if (accept) {
+                swap_state_with_y6();
+                r7_prev = r7_cur;
+                ++acc;
+            } else {
+                ++rej;
+            }
+        } while (!accept);
+    }
+
+    // ------------------------------------------------------------ FFT filter
+    void fft_filter() {
+        for (int q = 0; q < comps; ++q) {
+            if (!have_mask[q]) continue;
+            const long long N = (long long)N_r * N_c;
+            const int blocks = (int)std::min<long long>((N + 255) / 256, 148 * 16);
+            cudaEvent_t a = nullptr;
+            prof_begin(a);
+            gather_interior_kernel<T><<<blocks, 256, 0, stream>>>(cplane(psi[q]), pitch, N_r, N_c, reinterpret_cast<C*>(fft_x.p));
+            exec_fft(CUFFT_FORWARD);
+            mask_kernel<T><<<blocks, 256, 0, stream>>>(reinterpret_cast<C*>(fft_x.p), reinterpret_cast<const T*>(mask[q].p), N);
+            exec_fft(CUFFT_INVERSE);
+            scatter_interior_kernel<T><<<blocks, 256, 0, stream>>>(reinterpret_cast<C*>(fft_x.p), cplane(psi[q]), pitch, N_r, N_c,
+                                                                   P.periodic_x, P.periodic_y);
+            prof_end(PHX_KERNEL_FILTER, a, (double)N * (6 * sizeof(C) + sizeof(T)));
+            launches += 3;
+            PHX_CUDA(cudaGetLastError());
+        }
+    }
+    void exec_fft(int dir) {
+        if constexpr (sizeof(T) == 4) {
+            PHX_CUFFT(cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(fft_x.p), reinterpret_cast<cufftComplex*>(fft_x.p), dir));
+        } else {
+            PHX_CUFFT(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(fft_x.p),
+                                   reinterpret_cast<cufftDoubleComplex*>(fft_x.p), dir));
+        }
+    }
+
+    // ------------------------------------------------------------ iterate
+    void step(int64_t max_iterations, phx_step_info* info) override {
+        const int64_t l0 = launches;
+        int64_t its = 0, acc = 0, rej = 0, filt = 0;
+        const T t_max = (T)P.t_max, fft_every = (T)P.fft_every;
+        const bool dp45 = P.iterator == PHX_ITER_DP45;
+        while (its < max_iterations) {
+            if (t >= t_max) break;
+            update_kernel_time();
+            t = t + dt;
+            if (dp45) {
+                step_dp45(P.adaptive != 0, acc, rej);
+            } else {
+                step_rk4();
+            }
+            ++its;
+            if (t - fft_cached_t < fft_every) continue;
+            fft_cached_t = t;
+            if (have_mask[0] || have_mask[1]) {
+                fft_filter();
+                ++filt;
+            }
+        }
+        // RK4 work stays queued on the stream (no host sync); DP45 synchronised
+        // on every attempt already.  Reads of fields synchronise.
+        PHX_CUDA(cudaGetLastError());
+        if (info) {
+            info->t = (double)t;
+            info->dt = (double)dt;
+            info->iterations = its;
+            info->accepted = acc;
+            info->rejected = rej;
+            info->fft_filters = filt;
+            info->kernel_launches = launches - l0;
+        }
+    }
+
+    double sum_abs2(int field) override {
+        FieldRef f = field_ref(field, 0);
+        const int blocks = 296;
+        if (f.complex)
+            sum_abs2_kernel<T, true><<<blocks, 256, 0, stream>>>(reinterpret_cast<const T*>(cplane(*f.buf)), pitch, N_r, N_c,
+                                                                 reinterpret_cast<double*>(partials.p));
+        else
+            sum_abs2_kernel<T, false><<<blocks, 256, 0, stream>>>(rplane(*f.buf), pitch, N_r, N_c,
+                                                                  reinterpret_cast<double*>(partials.p));
+        finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), blocks,
+                                                      reinterpret_cast<double*>(result.p));
+        launches += 2;
+        PHX_CUDA(cudaGetLastError());
+        PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        return static_cast<const double*>(host_result.p)[0];
+    }
+};
+
+}  // namespace phx
+
+// ====================================================================== C ABI
+struct phx_handle {
+    std::unique_ptr<phx::EngineBase> eng;
+    std::string err;
+};
+
+namespace {
+
+phx_status guard(phx_handle* h, const std::function<void()>& f) {
+    try {
+        f();
+        if (h) h->err.clear();
+        return PHX_OK;
+    } catch (const phx::Error& e) {
+        if (h) h->err = e.msg;
+        else phx::g_create_error = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        if (h) h->err = "host allocation failed";
+        else phx::g_create_error = "host allocation failed";
+        return PHX_ERR_OOM;
+    } catch (const std::exception& e) {
+        if (h) h->err = e.what();
+        else phx::g_create_error = e.what();
+        return PHX_ERR_INVALID_ARG;
+    }
+}
+
+void validate(const phx_params& p) {
+    using phx::fail;
+    if (p.abi_version != PHX_ABI_VERSION) fail(PHX_ERR_INVALID_ARG, "abi_version mismatch");
+    if (p.N_c < 8 || p.N_r < 8) fail(PHX_ERR_INVALID_ARG, "grid must be at least 8 x 8");
+    if ((long long)p.N_c * p.N_r > (1LL << 31)) fail(PHX_ERR_INVALID_ARG, "grid too large");
+    if (p.dtype != PHX_F32 && p.dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "dtype must be PHX_F32 or PHX_F64");
+    if (p.dtype == PHX_F32 && (p.N_c & 1)) fail(PHX_ERR_UNSUPPORTED, "FP32 grids need an even N_c");
+    if (p.iterator != PHX_ITER_RK4 && p.iterator != PHX_ITER_DP45) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
+    if (p.adaptive && p.iterator != PHX_ITER_DP45) fail(PHX_ERR_INVALID_ARG, "adaptive stepping needs DP45");
+    if (p.norm_mode != PHX_NORM_REFERENCE && p.norm_mode != PHX_NORM_INTERIOR) fail(PHX_ERR_INVALID_ARG, "bad norm_mode");
+    if (!(p.L_x > 0) || !(p.L_y > 0) || !(p.h_bar_s > 0) || !(p.m_eff > 0)) fail(PHX_ERR_INVALID_ARG, "L, h_bar_s and m_eff must be > 0");
+    if (!(p.dt > 0)) fail(PHX_ERR_INVALID_ARG, "dt must be > 0");
+    if (p.n_pump_groups < 0 || p.n_pump_groups > phx::kMaxGroups || p.n_potential_groups < 0 ||
+        p.n_potential_groups > phx::kMaxGroups || p.n_pulse_groups < 0 || p.n_pulse_groups > phx::kMaxGroups)
+        fail(PHX_ERR_INVALID_ARG, "temporal group count out of range (0..8)");
+    if (p.n_pump_groups > 0 && !p.use_reservoir) fail(PHX_ERR_INVALID_ARG, "pump groups need use_reservoir");
+    if (p.tetm && !p.use_reservoir) fail(PHX_ERR_UNSUPPORTED, "TE/TM mode reads the reservoir; set use_reservoir");
+    if (p.stochastic_amplitude != 0.0) fail(PHX_ERR_UNSUPPORTED, "stochastic noise is not available in this build");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        fail(PHX_ERR_CUDA, "no CUDA device available");
+    }
+    if (p.device < 0 || p.device >= ndev) fail(PHX_ERR_INVALID_ARG, "device ordinal out of range");
+}
+
+}  // namespace
+
+extern "C" {
+
+phx_status phx_create(const phx_params* p, phx_handle** out) {
+    if (!p || !out) {
+        phx::g_create_error = "NULL argument";
+        return PHX_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    std::unique_ptr<phx_handle> h(new (std::nothrow) phx_handle());
+    if (!h) return PHX_ERR_OOM;
+    phx_status st = guard(nullptr, [&] {
+        validate(*p);
+        if (p->dtype == PHX_F64)
+            h->eng.reset(new phx::Engine<double>());
+        else
+            h->eng.reset(new phx::Engine<float>());
+        h->eng->P = *p;
+        h->eng->init();
+    });
+    if (st != PHX_OK) return st;
+    *out = h.release();
+    return PHX_OK;
+}
+
+phx_status phx_destroy(phx_handle* h) {
+    if (!h) return PHX_OK;
+    if (h->eng) {
+        cudaSetDevice(h->eng->P.device);
+        if (h->eng->stream) cudaStreamSynchronize(h->eng->stream);
+    }
+    delete h;
+    return PHX_OK;
+}
+
+phx_status phx_set_field(phx_handle* h, int32_t field, int32_t group, const void* host, int64_t count, int32_t host_dtype) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->set_field(field, group, host, count, host_dtype); });
+}
+
+phx_status phx_get_field(phx_handle* h, int32_t field, int32_t group, void* host, int64_t count, int32_t host_dtype) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->get_field(field, group, host, count, host_dtype); });
+}
+
+phx_status phx_set_temporal(phx_handle* h, int32_t envelope, int32_t group, int32_t kind, double t0, double sigma, double freq) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (kind < PHX_TEMPORAL_CONSTANT || kind > PHX_TEMPORAL_GAUSS) phx::fail(PHX_ERR_INVALID_ARG, "unknown temporal kind");
+        phx::TemporalSpec s;
+        s.kind = kind;
+        s.t0 = t0;
+        s.sigma = sigma;
+        s.freq = freq;
+        auto& P = h->eng->P;
+        if (envelope == PHX_ENV_PUMP) {
+            if (group < 0 || group >= P.n_pump_groups) phx::fail(PHX_ERR_INVALID_ARG, "pump group out of range");
+            if (kind == PHX_TEMPORAL_IEXP) phx::fail(PHX_ERR_UNSUPPORTED, "complex (iexp) pump envelopes make the reservoir complex");
+            h->eng->pump_t[group] = s;
+        } else if (envelope == PHX_ENV_POTENTIAL) {
+            if (group < 0 || group >= P.n_potential_groups) phx::fail(PHX_ERR_INVALID_ARG, "potential group out of range");
+            h->eng->pot_t[group] = s;
+        } else if (envelope == PHX_ENV_PULSE) {
+            if (group < 0 || group >= P.n_pulse_groups) phx::fail(PHX_ERR_INVALID_ARG, "pulse group out of range");
+            h->eng->pulse_t[group] = s;
+        } else {
+            phx::fail(PHX_ERR_INVALID_ARG, "unknown envelope family");
+        }
+    });
+}
+
+phx_status phx_step(phx_handle* h, int64_t max_iterations, phx_step_info* info) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (max_iterations < 0) phx::fail(PHX_ERR_INVALID_ARG, "max_iterations < 0");
+        h->eng->step(max_iterations, info);
+    });
+}
+
+phx_status phx_get_time(phx_handle* h, double* t, double* dt) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->get_time(t, dt); });
+}
+
+phx_status phx_set_time(phx_handle* h, double t, double dt) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (!(dt > 0)) phx::fail(PHX_ERR_INVALID_ARG, "dt must be > 0");
+        h->eng->set_time(t, dt);
+    });
+}
+
+phx_status phx_sum_abs2(phx_handle* h, int32_t field, double* out) {
+    if (!h || !out) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (field != PHX_PSI_PLUS && field != PHX_PSI_MINUS && field != PHX_N_PLUS && field != PHX_N_MINUS)
+            phx::fail(PHX_ERR_INVALID_ARG, "sum_abs2 takes a state field");
+        *out = h->eng->sum_abs2(field);
+    });
+}
+
+phx_status phx_field_device_ptr(phx_handle* h, int32_t field, int32_t group, void** dev_ptr, int64_t* row_pitch_elems) {
+    if (!h || !dev_ptr) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->field_ptr(field, group, dev_ptr, row_pitch_elems); });
+}
+
+phx_status phx_profile_enable(phx_handle* h, int32_t enable) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        h->eng->prof_reset();
+        h->eng->profiling = enable != 0;
+    });
+}
+
+phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (kind < 0 || kind >= PHX_KERNEL_KINDS) phx::fail(PHX_ERR_INVALID_ARG, "unknown kernel kind");
+        h->eng->prof_harvest();
+        if (total_ms) *total_ms = h->eng->prof_ms[kind];
+        if (launches) *launches = h->eng->prof_count[kind];
+        if (bytes) *bytes = h->eng->prof_bytes[kind];
+    });
+}
+
+phx_status phx_get_stream(phx_handle* h, void** stream) {
+    if (!h || !stream) return PHX_ERR_INVALID_ARG;
+    *stream = (void*)h->eng->stream;
+    return PHX_OK;
+}
+
+const char* phx_last_error(const phx_handle* h) {
+    if (!h) return phx::g_create_error.c_str();
+    return h->err.c_str();
+}
+
+const char* phx_status_string(int32_t s) {
+    switch (s) {
+        case PHX_OK: return "ok";
+        case PHX_ERR_INVALID_ARG: return "invalid argument";
+        case PHX_ERR_OOM: return "out of memory";
+        case PHX_ERR_CUDA: return "CUDA error";
+        case PHX_ERR_NONFINITE: return "non-finite value";
+        case PHX_ERR_TIMEOUT: return "timeout";
+        case PHX_ERR_UNSUPPORTED: return "unsupported";
+        case PHX_ERR_STATE: return "invalid state";
+        default: return "unknown status";
+    }
+}
+
+int32_t phx_abi_version(void) { return PHX_ABI_VERSION; }
+
+const char* phx_build_info(void) { return "phx-b200 sm_100a fused-stage RK4/DP45 (nvcc " PHX_NVCC_VERSION ")"; }
+
+}  // extern "C"

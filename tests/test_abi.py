@@ -1,0 +1,58 @@
+"""The C ABI library: it loads without a GPU, exports every function that
+include/phx.h declares, and rejects bad arguments before touching a device."""
+import ctypes as C
+
+import pytest
+
+import phoenix_b200 as pb
+from phoenix_b200 import _lib as L
+
+
+def test_header_declares_the_abi():
+    names = L.header_symbols()
+    for required in ("phx_create", "phx_destroy", "phx_set_field", "phx_get_field", "phx_set_temporal", "phx_step",
+                     "phx_get_time", "phx_set_time", "phx_sum_abs2", "phx_field_device_ptr", "phx_last_error"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load()
+    for name in L.header_symbols():
+        assert hasattr(lib, name), f"{name} declared in include/phx.h but not exported"
+
+
+def test_abi_version_and_build_info():
+    lib = L.load()
+    assert lib.phx_abi_version() == L.ABI_VERSION
+    assert b"sm_100a" in lib.phx_build_info()
+
+
+def test_status_strings():
+    lib = L.load()
+    assert lib.phx_status_string(0) == b"ok"
+    assert lib.phx_status_string(6) == b"unsupported"
+
+
+def test_create_rejects_bad_parameters_without_device_work():
+    lib = L.load()
+    h = C.c_void_p()
+    p = pb.SystemParameters(N_c=4, N_r=4, dt=0.01).to_abi()
+    st = lib.phx_create(C.byref(p), C.byref(h))
+    assert st == 1 and not h.value
+    assert b"8 x 8" in lib.phx_last_error(None)
+    p = pb.SystemParameters(N_c=32, N_r=32, dt=0.01).to_abi()
+    p.abi_version = 99
+    assert lib.phx_create(C.byref(p), C.byref(h)) == 1
+    p = pb.SystemParameters(N_c=33, N_r=32, dt=0.01, dtype="f32").to_abi()
+    assert lib.phx_create(C.byref(p), C.byref(h)) == 6
+
+
+def test_null_handle_calls_fail_cleanly():
+    lib = L.load()
+    assert lib.phx_step(None, 1, None) == 1
+    assert lib.phx_destroy(None) == 0
+
+
+def test_unknown_iterator_is_rejected_like_the_factory():
+    with pytest.raises(KeyError):
+        pb.SystemParameters(iterator="RK17").to_abi()

@@ -1,0 +1,131 @@
+"""GPU parity through the C ABI against the reference's own outputs.
+
+Every golden fixture (tests/golden/*.npz, written by the PHOENIX CPU build)
+is replayed through phoenix_b200 -> libphx.so on the GPU.  The kernels use
+explicitly rounded operations in the reference's operand order, so FP64 and
+FP32 results are expected to be bit-identical to the reference CPU build;
+the asserted bounds are the north star's (rel-L2 <= 1e-12 for FP64) and
+1e-6 for FP32.  The k-space filter goes through cuFFT instead of FFTW, and
+DP45 sums its norms in FP64 instead of the build precision, so those cases
+are held to the bound, not to bit equality.
+"""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+import phoenix_b200 as pb
+from oracle import phx_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+SUPPORTED = GOLDEN
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def run_gpu(case, fields, **over):
+    sp = pb.system_from_case(case, **over)
+    with pb.SolverFactory.create(sp) as s:
+        pb.load_case_fields(s, case, fields)
+        info = s.run()
+        comps = ["plus", "minus"] if sp.use_twin_mode else ["plus"]
+        out = {}
+        for c in comps:
+            out[f"psi_{c}"] = s.get_field(f"psi_{c}")
+            if sp.use_reservoir:
+                out[f"n_{c}"] = s.get_field(f"n_{c}")
+        return out, info, s.t
+
+
+@pytest.mark.parametrize("path", SUPPORTED, ids=[os.path.basename(p)[:-4] for p in SUPPORTED])
+def test_gpu_matches_reference_golden(require_gpu, path):
+    z = np.load(path)
+    case = json.loads(str(z["params"]))
+    fields = O.fields_from_golden(z)
+    out, info, t = run_gpu(case, fields)
+    _, rec = O.run(case, fields)
+    assert info.iterations == rec["steps"]
+    assert info.kernel_launches > 0
+    tol = 1e-12 if case["dtype"] == "f64" else 1e-6
+    for k in ("psi_plus", "n_plus", "psi_minus", "n_minus"):
+        gk = "out_" + k
+        if gk not in z.files or k not in out:
+            continue
+        ref = z[gk] if k.startswith("psi") else np.real(z[gk])
+        err = rel_l2(out[k], ref)
+        assert err <= tol, f"{k}: rel-L2 {err:.3e} > {tol}"
+        exact = not case.get("mask_cut") and not case.get("adaptive")
+        if exact:
+            np.testing.assert_array_equal(out[k], ref, err_msg=f"{k} not bit-identical to the reference")
+
+
+def test_config1_256_fp64_1000_steps_matches_oracle(require_gpu):
+    """North-star parity: 256^2 periodic, FP64, RK4, dt 0.04, 1000 steps, Gaussian
+    pump at 1.5x threshold, complex white-noise psi0 of amplitude 1e-2."""
+    N, L = 256, 100.0
+    rng = np.random.default_rng(1)
+    x = -L / 2 + L / (N - 1) * np.arange(N)
+    X, Y = np.meshgrid(x, x)
+    pth = 0.15 * 0.225 / 0.01
+    case = dict(N_c=N, N_r=N, L_x=L, L_y=L, h_bar_s=0.6582, m_eff=3.1840, gamma_c=0.15, gamma_r=0.225, g_c=6e-6,
+                g_r=1.2e-5, R=0.01, g_pm=0.0, delta_LT=0.0, dtype="f64", iterator="RK4", dt=0.04,
+                t_max=1000 * 0.04 * (1 - 1e-9), periodic_x=1, periodic_y=1, pumps=[(1.5 * pth, 10.0, 0.0)])
+    fields = {"psi_plus": 1e-2 * (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))),
+              "pump_0": 1.5 * pth * np.exp(-(X ** 2 + Y ** 2) / (2 * 10.0 ** 2))}
+    out, info, t = run_gpu(case, fields)
+    ref, rec = O.run(case, fields)
+    assert info.iterations == rec["steps"] == 1000
+    for k in ("psi_plus", "n_plus"):
+        r = ref[k] if k.startswith("psi") else np.real(ref[k])
+        err = rel_l2(out[k], r)
+        assert err <= 1e-12, f"{k}: rel-L2 {err:.3e}"
+
+
+def test_periodic_translation_equivariance_1024_fp32(require_gpu):
+    """Full-size property: with periodic boundaries a cyclic shift of every input
+    field shifts the result by the same amount, bit for bit."""
+    N = 1024
+    rng = np.random.default_rng(3)
+    psi = 0.1 * (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N)))
+    pump = 5.0 * rng.random((N, N))
+    pot = 0.1 * rng.standard_normal((N, N))
+    sp = pb.SystemParameters(N_c=N, N_r=N, L_x=100.0, L_y=100.0, h_bar_s=0.6582, m_eff=3.184, g_c=6e-6, g_r=1.2e-5,
+                             periodic_boundary_x=True, periodic_boundary_y=True, dtype="f32", dt=0.02, t_max=1e9,
+                             fft_every=1e9, pump_temporal=[pb.Temporal()], potential_temporal=[pb.Temporal()])
+    shift = (37, 501)
+    res = []
+    for s_ in ((0, 0), shift):
+        with pb.Solver(sp) as s:
+            s.set_field("psi_plus", np.roll(psi, s_, (0, 1)))
+            s.set_field("n_plus", np.zeros((N, N)))
+            s.set_field("pump_plus", np.roll(pump, s_, (0, 1)))
+            s.set_field("potential_plus", np.roll(pot, s_, (0, 1)))
+            s.run(20)
+            res.append(s.get_field("psi_plus"))
+    np.testing.assert_array_equal(np.roll(res[0], shift, (0, 1)), res[1])
+
+
+def test_fp32_vs_fp64_error_is_bounded(require_gpu):
+    """FP32 error against the FP64 path on the 64^2 baseline-physics golden case."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "rk4_f64_baseline_phys.npz"))
+    case = json.loads(str(z["params"]))
+    fields = O.fields_from_golden(z)
+    o64, _, _ = run_gpu(case, fields)
+    o32, _, _ = run_gpu(dict(case, dtype="f32"), fields)
+    err = rel_l2(o32["psi_plus"], o64["psi_plus"])
+    assert err < 1e-5, err
+
+
+def test_bad_field_shape_is_rejected(require_gpu):
+    sp = pb.SystemParameters(N_c=32, N_r=32, dt=0.01)
+    with pb.Solver(sp) as s:
+        with pytest.raises(ValueError):
+            s.set_field("psi_plus", np.zeros((16, 16)))
+        with pytest.raises(pb.PhxError):
+            s.get_field("pump_plus", 0)  # no pump groups configured
