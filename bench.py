@@ -43,7 +43,15 @@ sys.path.insert(0, ROOT)
 N_DEFAULT = 1024
 L_BOX = 100.0
 PHYS = dict(h_bar_s=0.6582, m_eff=3.1840, gamma_c=0.15, gamma_r=0.225, g_c=6e-6, g_r=1.2e-5, R=0.01)
-DT = 0.02
+DT_1024 = 0.02  # ps; RK4 stability at 1024^2 with m_eff = 5.6e-4 m_e needs dt < 0.033
+
+
+def dt_for(n):
+    """0.02 ps at 1024^2, scaled with dx^2 for other grids (0.00125 ps at 4096^2)."""
+    return min(0.04, DT_1024 * (1024.0 / n) ** 2)
+
+
+DT = DT_1024
 MASK_EVERY = 100
 P_TH = 0.15 * 0.225 / 0.01
 METRIC = "us_per_rk4_iteration_1024x1024"
@@ -68,9 +76,10 @@ def workload(n, seed=2):
 
 
 def system(pb, n, dtype, device):
+    dt = dt_for(n)
     return pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
-                               periodic_boundary_y=True, dtype=dtype, iterator="RK4", dt=DT, t0=0.0, t_max=1e12,
-                               fft_every=MASK_EVERY * DT * (1 - 1e-6), pump_temporal=[pb.Temporal()],
+                               periodic_boundary_y=True, dtype=dtype, iterator="RK4", dt=dt, t0=0.0, t_max=1e12,
+                               fft_every=MASK_EVERY * dt * (1 - 1e-6), pump_temporal=[pb.Temporal()],
                                potential_temporal=[pb.Temporal()], device=device)
 
 
@@ -145,13 +154,14 @@ def reference_cpu_run(n, dtype, iters, wl):
         for key in ("psi0", "pump", "potential", "mask"):
             files[key] = os.path.join(tmp, key + ".txt")
             write_txt(files[key], wl[key])
-        t_max = iters * DT * (1 - 1e-9)
-        args = [binary, "--N", str(n), str(n), "--L", str(L_BOX), str(L_BOX), "--dt", str(DT), "--tmax", repr(t_max),
+        dt = dt_for(n)
+        t_max = iters * dt * (1 - 1e-9)
+        args = [binary, "--N", str(n), str(n), "--L", str(L_BOX), str(L_BOX), "--dt", repr(dt), "--tmax", repr(t_max),
                 "--outEvery", "1e9", "--output", "none", "--path", os.path.join(tmp, "out"), "--threads", str(cores),
                 "--boundary", "periodic", "periodic", "--hbarscaled", str(PHYS["h_bar_s"]), "--meff",
                 str(PHYS["m_eff"]), "--gammaC", str(PHYS["gamma_c"]), "--gammaR", str(PHYS["gamma_r"]), "--gc",
                 str(PHYS["g_c"]), "--gr", str(PHYS["g_r"]), "--R", str(PHYS["R"]), "--fftEvery",
-                repr(MASK_EVERY * DT * (1 - 1e-6)), "--initState", "load", files["psi0"], "1", "add", "both",
+                repr(MASK_EVERY * dt * (1 - 1e-6)), "--initState", "load", files["psi0"], "1", "add", "both",
                 "--pump", "load", files["pump"], "1", "add", "both", "--potential", "load", files["potential"], "1",
                 "add", "both", "--fftMask", "load", files["mask"], "1", "add", "both"]
         proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
@@ -166,8 +176,8 @@ def oracle_port_run(n, dtype, iters, wl):
     from oracle import phx_oracle as O
 
     case = dict(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, g_pm=0.0, delta_LT=0.0, dtype=dtype, iterator="RK4",
-                dt=DT, t_max=1e12, periodic_x=1, periodic_y=1, pumps=[(0, 0, 0)], potentials=[0.0],
-                mask_cut=0.8, fft_every=MASK_EVERY * DT * (1 - 1e-6))
+                dt=dt_for(n), t_max=1e12, periodic_x=1, periodic_y=1, pumps=[(0, 0, 0)], potentials=[0.0],
+                mask_cut=0.8, fft_every=MASK_EVERY * dt_for(n) * (1 - 1e-6))
     fields = {"psi_plus": wl["psi0"], "pump_0": wl["pump"], "potential_0": wl["potential"], "fft_mask": wl["mask"]}
     t0 = time.perf_counter()
     O.run(case, fields, max_steps=iters)
@@ -200,7 +210,7 @@ def run_reference_arm(args):
 
 def config_dict(args):
     return {"workload": f"rk4_scalar_reservoir_pump_potential_mask_{args.n}x{args.n}_{args.dtype}",
-            "grid": [args.n, args.n], "iterator": "RK4", "boundary": "periodic", "dt_ps": DT,
+            "grid": [args.n, args.n], "iterator": "RK4", "boundary": "periodic", "dt_ps": dt_for(args.n),
             "mask_every_iterations": MASK_EVERY, "physics": "polariton GP + reservoir, meV/ps/um, hbar 0.6582, "
             "m_eff 5.6e-4 m_e", "replicas": "one independent simulation per GPU",
             "l2": "256 MiB write between timed iterations (value); e2e runs back to back"}
@@ -270,6 +280,7 @@ def main():
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     launches = 0
     filters = 0
+    shape = -1
     solver.profile(True)
     with ClockSampler(smi_index) as clocks:
         for i in range(args.steps):
@@ -279,6 +290,7 @@ def main():
             info = solver.run(1)
             with torch.cuda.stream(stream):
                 ends[i].record(stream)
+            shape = info.launch_shape
             launches += info.kernel_launches
             filters += info.fft_filters
         torch.cuda.synchronize()
@@ -388,7 +400,7 @@ def main():
                              "peak_source": peak_src, "bytes_per_launch": per_launch_bytes,
                              "step_alg_bytes": step_bytes,
                              "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},
-                "kernel_avg_ms": kernels_ms, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
+                "kernel_avg_ms": kernels_ms, "launch_shape": shape, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
                 "clocks": clocks.summary(), "cpu_baseline": cpu}
         print(json.dumps(line))
     if dist:

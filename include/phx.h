@@ -117,6 +117,8 @@ typedef struct {
     int64_t accepted, rejected;     /* DP45 attempts */
     int64_t fft_filters;            /* k-space mask applications */
     int64_t kernel_launches;        /* this library's kernels launched */
+    int32_t launch_shape;           /* stage-kernel launch shape in use (-1 while tuning) */
+    int32_t reserved;
 } phx_step_info;
 
 typedef struct phx_handle phx_handle;

@@ -53,7 +53,8 @@ class Params(C.Structure):
 
 class StepInfo(C.Structure):
     _fields_ = [("t", C.c_double), ("dt", C.c_double), ("iterations", C.c_int64), ("accepted", C.c_int64),
-                ("rejected", C.c_int64), ("fft_filters", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("rejected", C.c_int64), ("fft_filters", C.c_int64), ("kernel_launches", C.c_int64),
+                ("launch_shape", C.c_int32), ("reserved", C.c_int32)]
 
 
 _lib = None

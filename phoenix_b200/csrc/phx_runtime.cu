@@ -15,6 +15,7 @@
 #include <limits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -161,7 +162,9 @@ template <typename T>
 struct Engine final : EngineBase {
     static constexpr int G = kRing;
     static constexpr int CPT = Pack<T>::CPT;
-    static constexpr int RB = 8;
+    int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
+    int tune_step = 0;              // steps run while tuning
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes];
     static constexpr int kRingBlocks = 64;
     using C = cx<T>;
 
@@ -234,7 +237,13 @@ struct Engine final : EngineBase {
             pot[q].alloc(rb * std::max(1, P.n_potential_groups), stream);
             pulse[q].alloc(cb * std::max(1, P.n_pulse_groups), stream);
         }
-        const long long max_blocks = grid_x(-(long long)G, N_c + G) * grid_y(-(long long)G, N_r + G) + 64;
+        long long min_rpb = rows_per_block(0);
+        for (int sh = 1; sh < kShapes; ++sh) min_rpb = std::min(min_rpb, rows_per_block(sh));
+        const long long max_blocks = grid_x(-(long long)G, N_c + G) * ((N_r + 2LL * G + min_rpb - 1) / min_rpb) + 64;
+        if (const char* e = std::getenv("PHX_STAGE_SHAPE")) {
+            const int v = std::atoi(e);
+            if (v >= 0 && v < kShapes) shape = v;
+        }
         partials.alloc(sizeof(double) * 2 * std::max<long long>(max_blocks, 1024), stream);
         result.alloc(sizeof(double) * 4, stream);
         host_result.alloc(sizeof(double) * 4);
@@ -245,7 +254,12 @@ struct Engine final : EngineBase {
     }
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
-    long long grid_y(long long r0, long long r1) const { return (r1 - r0 + kStageWarps * RB - 1) / (kStageWarps * RB); }
+    int cur_shape() const { return shape >= 0 ? shape : tune_step % kShapes; }
+    long long rows_per_block(int sh) const { return (long long)kShapeRB[sh] * kShapeWarps[sh]; }
+    long long grid_y(long long r0, long long r1) const {
+        const long long rpb = rows_per_block(cur_shape());
+        return (r1 - r0 + rpb - 1) / rpb;
+    }
 
     // ------------------------------------------------------------ fields
     struct FieldRef {
@@ -479,14 +493,27 @@ struct Engine final : EngineBase {
         }
         return b * (double)(S.r1 - S.r0) * (double)(S.c1 - S.c0);
     }
+    template <int KIND, bool RES, int SH>
+    void go_scalar(const StageParams<T>& S, dim3 grid) {
+        stage_scalar_kernel<T, KIND, RES, kShapeRB[SH], kShapeWarps[SH]><<<grid, 32 * kShapeWarps[SH], 0, stream>>>(S);
+    }
     template <int KIND, bool RES>
     void launch_kind(const StageParams<T>& S) {
         dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
         cudaEvent_t a = nullptr;
         prof_begin(a);
-        stage_scalar_kernel<T, KIND, RES, RB><<<grid, 32 * kStageWarps, 0, stream>>>(S);
+        switch (cur_shape()) {
+            case 0: go_scalar<KIND, RES, 0>(S, grid); break;
+            case 1: go_scalar<KIND, RES, 1>(S, grid); break;
+            case 2: go_scalar<KIND, RES, 2>(S, grid); break;
+            default: go_scalar<KIND, RES, 3>(S, grid); break;
+        }
         prof_end(KIND, a, stage_bytes(KIND, RES, S));
         ++launches;
+    }
+    template <int KIND, int SH>
+    void go_tetm(const TetmParams<T>& Q, dim3 grid) {
+        stage_tetm_kernel<T, KIND, kShapeRB[SH], kShapeWarps[SH]><<<grid, 32 * kShapeWarps[SH], 0, stream>>>(Q);
     }
     // Launch stage KIND.  `wire(S, q)` points S at component q's planes; in
     // TE/TM mode the minus component's planes are wired the same way and
@@ -511,7 +538,12 @@ struct Engine final : EngineBase {
             dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
             cudaEvent_t a = nullptr;
             prof_begin(a);
-            stage_tetm_kernel<T, KIND, RB><<<grid, 32 * kStageWarps, 0, stream>>>(Q);
+            switch (cur_shape()) {
+                case 0: go_tetm<KIND, 0>(Q, grid); break;
+                case 1: go_tetm<KIND, 1>(Q, grid); break;
+                case 2: go_tetm<KIND, 2>(Q, grid); break;
+                default: go_tetm<KIND, 3>(Q, grid); break;
+            }
             prof_end(KIND, a, 2 * stage_bytes(KIND, true, S));
             ++launches;
         } else if (P.use_reservoir) {
@@ -784,11 +816,17 @@ struct Engine final : EngineBase {
             if (t >= t_max) break;
             update_kernel_time();
             t = t + dt;
+            cudaEvent_t ta = nullptr, tb = nullptr;
+            if (shape < 0) {
+                ta = get_event();
+                PHX_CUDA(cudaEventRecord(ta, stream));
+            }
             if (dp45) {
                 step_dp45(P.adaptive != 0, acc, rej);
             } else {
                 step_rk4();
             }
+            if (shape < 0) tune_record(ta, tb);
             ++its;
             if (t - fft_cached_t < fft_every) continue;
             fft_cached_t = t;
@@ -808,7 +846,39 @@ struct Engine final : EngineBase {
             info->rejected = rej;
             info->fft_filters = filt;
             info->kernel_launches = launches - l0;
+            info->launch_shape = shape;
+            info->reserved = 0;
         }
+    }
+
+    // Launch-shape autotuning: the first 2*kShapes iterations of a handle run
+    // with each shape twice (results do not depend on the shape: every point
+    // is computed by the same operations); the second round is timed and the
+    // fastest shape is kept.
+    void tune_record(cudaEvent_t ta, cudaEvent_t tb) {
+        tb = get_event();
+        PHX_CUDA(cudaEventRecord(tb, stream));
+        tune_ev[tune_step % kShapes].push_back({ta, tb});
+        ++tune_step;
+        if (tune_step < 2 * kShapes) return;
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        float best = 1e30f;
+        int best_sh = kDefaultShape;
+        for (int sh = 0; sh < kShapes; ++sh) {
+            float ms = 1e30f;
+            for (size_t i = 1; i < tune_ev[sh].size(); ++i) {
+                float m = 0.f;
+                PHX_CUDA(cudaEventElapsedTime(&m, tune_ev[sh][i].first, tune_ev[sh][i].second));
+                ms = std::min(ms, m);
+            }
+            if (ms < best) best = ms, best_sh = sh;
+            for (auto& pr : tune_ev[sh]) {
+                event_pool.push_back(pr.first);
+                event_pool.push_back(pr.second);
+            }
+            tune_ev[sh].clear();
+        }
+        shape = best_sh;
     }
 
     double sum_abs2(int field) override {

@@ -17,6 +17,14 @@
 
 namespace phx {
 
+// Launch shapes (rows per warp, warps per block) the stage kernels are
+// instantiated for; the runtime times them on the first steps of a handle
+// and keeps the fastest.
+constexpr int kShapes = 4;
+constexpr int kShapeRB[kShapes] = {1, 2, 4, 8};
+constexpr int kShapeWarps[kShapes] = {8, 8, 4, 4};
+constexpr int kDefaultShape = 0;
+
 enum StageKind : int {
     kRk4First = 0,  // k1 = f(y0); A = b1 k1; y1 = y0 + (dt a) k1
     kRk4Mid = 1,    // k = f(y_s); A += b k;  y_{s+1} = y0 + (dt a) k
@@ -194,17 +202,16 @@ __device__ __forceinline__ void block_reduce2(double& a, double& b, double* smem
     }
 }
 
-constexpr int kStageWarps = 4;
-
-// Launch: block (32*kStageWarps), grid (ceil(W / (32*CPT)), ceil(H / (kStageWarps*RB))).
-template <typename T, int KIND, bool RES, int RB>
-__global__ void __launch_bounds__(32 * kStageWarps) stage_scalar_kernel(const __grid_constant__ StageParams<T> P) {
+// Launch: block (32*WARPS), grid (ceil(W / (32*CPT)), ceil(H / (WARPS*RB))).
+// Each warp owns RB consecutive rows of 32*CPT columns.
+template <typename T, int KIND, bool RES, int RB, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_constant__ StageParams<T> P) {
     constexpr int CPT = Pack<T>::CPT;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int c_base = P.c0 + blockIdx.x * (32 * CPT);
     const int c = c_base + lane * CPT;
-    const int rs = P.r0 + (blockIdx.y * kStageWarps + warp) * RB;
+    const int rs = P.r0 + (blockIdx.y * WARPS + warp) * RB;
     const int re = min(rs + RB, P.r1);
     const bool active = c < P.c1;
     const int cl = min(c, P.c1);  // columns [c1, c1+CPT) are allocated, so clamped loads stay in bounds
@@ -351,8 +358,8 @@ __global__ void __launch_bounds__(32 * kStageWarps) stage_scalar_kernel(const __
         }
     }
     if constexpr (KIND == kStackError) {
-        __shared__ double red[2 * kStageWarps];
-        block_reduce2<32 * kStageWarps>(err_acc, norm_acc, red);
+        __shared__ double red[2 * WARPS];
+        block_reduce2<32 * WARPS>(err_acc, norm_acc, red);
         if (threadIdx.x == 0) {
             const long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
             P.partials[2 * b] = err_acc;

@@ -134,15 +134,15 @@ __device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, 
     krm = r;
 }
 
-template <typename T, int KIND, int RB>
-__global__ void __launch_bounds__(32 * kStageWarps) stage_tetm_kernel(const __grid_constant__ TetmParams<T> Q) {
+template <typename T, int KIND, int RB, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_constant__ TetmParams<T> Q) {
     constexpr int CPT = Pack<T>::CPT;
     const StageParams<T>& P = Q.p;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int c_base = P.c0 + blockIdx.x * (32 * CPT);
     const int c = c_base + lane * CPT;
-    const int rs = P.r0 + (blockIdx.y * kStageWarps + warp) * RB;
+    const int rs = P.r0 + (blockIdx.y * WARPS + warp) * RB;
     const int re = min(rs + RB, P.r1);
     const bool active = c < P.c1;
     const int cl = min(c, P.c1);
@@ -307,8 +307,8 @@ __global__ void __launch_bounds__(32 * kStageWarps) stage_tetm_kernel(const __gr
         }
     }
     if constexpr (KIND == kStackError) {
-        __shared__ double red[2 * kStageWarps];
-        block_reduce2<32 * kStageWarps>(err_acc, norm_acc, red);
+        __shared__ double red[2 * WARPS];
+        block_reduce2<32 * WARPS>(err_acc, norm_acc, red);
         if (threadIdx.x == 0) {
             const long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
             P.partials[2 * b] = err_acc;
