@@ -117,7 +117,8 @@ typedef struct {
     int64_t accepted, rejected;     /* DP45 attempts */
     int64_t fft_filters;            /* k-space mask applications */
     int64_t kernel_launches;        /* this library's kernels launched */
-    int32_t launch_shape;           /* stage-kernel launch shape in use (-1 while tuning) */
+    int32_t launch_shape;           /* launch shape in use: 0-3 per-stage kernels, 4 fused RK4
+                                       iteration, -1 while the first iterations time them */
     int32_t reserved;
 } phx_step_info;
 
@@ -178,7 +179,8 @@ typedef enum {
     PHX_KERNEL_STAGE_ERROR = 5, /* DP45 k7 + error / norm reduction          */
     PHX_KERNEL_FILTER = 6,      /* k-space filter passes (without cuFFT)     */
     PHX_KERNEL_OTHER = 7,       /* rings, reductions                         */
-    PHX_KERNEL_KINDS = 8
+    PHX_KERNEL_RK4_FUSED = 8,   /* whole RK4 iteration in one launch         */
+    PHX_KERNEL_KINDS = 9
 } phx_kernel_kind;
 
 /* Per-launch CUDA-event timing of this handle's kernels (no reference

@@ -28,7 +28,7 @@ TEMPORAL = {"constant": 0, "iexp": 1, "osc": 1, "cos": 2, "gauss": 3}
 ENVELOPE = {"pump": 0, "potential": 1, "pulse": 2}
 ABI_VERSION = 1
 KERNEL_KINDS = {"rk4_first": 0, "rk4_mid": 1, "rk4_last": 2, "stage": 3, "stage_final": 4, "stage_error": 5,
-                "filter": 6, "other": 7}
+                "filter": 6, "other": 7, "rk4_fused": 8}
 
 
 class PhxError(RuntimeError):

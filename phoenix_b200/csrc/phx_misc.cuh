@@ -67,7 +67,7 @@ __global__ void mask_kernel(cx<T>* __restrict__ data, const T* __restrict__ mask
     }
 }
 
-// contiguous -> padded interior, plus ring-1 periodic images
+// contiguous -> padded interior, plus periodic images
 template <typename T>
 __global__ void scatter_interior_kernel(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, long long pitch, int N_r,
                                         int N_c, int periodic_x, int periodic_y) {
@@ -76,10 +76,12 @@ __global__ void scatter_interior_kernel(const cx<T>* __restrict__ src, cx<T>* __
         const int r = (int)(i / N_c), c = (int)(i % N_c);
         const cx<T> v = src[i];
         dst[(long long)r * pitch + c] = v;
-        const bool ex = periodic_x && (c == 0 || c == N_c - 1);
-        const bool ey = periodic_y && (r == 0 || r == N_r - 1);
-        const int ci = c == 0 ? N_c : -1;
-        const int ri = r == 0 ? N_r : -1;
+        // periodic images four deep, as the stage kernels write them
+        const bool lx = periodic_x && c < 4, hx = periodic_x && c >= N_c - 4;
+        const bool ly = periodic_y && r < 4, hy = periodic_y && r >= N_r - 4;
+        const bool ex = lx || hx, ey = ly || hy;
+        const int ci = lx ? c + N_c : c - N_c;
+        const int ri = ly ? r + N_r : r - N_r;
         if (ex) dst[(long long)r * pitch + ci] = v;
         if (ey) dst[(long long)ri * pitch + c] = v;
         if (ex && ey) dst[(long long)ri * pitch + ci] = v;

@@ -27,6 +27,7 @@
 #include "phx_misc.cuh"
 #include "phx_stage.cuh"
 #include "phx_stage_tetm.cuh"
+#include "phx_step_fused.cuh"
 
 namespace phx {
 
@@ -164,7 +165,7 @@ struct Engine final : EngineBase {
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 1];
     static constexpr int kRingBlocks = 64;
     using C = cx<T>;
 
@@ -182,6 +183,7 @@ struct Engine final : EngineBase {
     DevBuf pump[2], pot[2], pulse[2];  // input planes (groups)
     DevBuf mask[2];                    // fft-shifted mask, contiguous N_r*N_c
     DevBuf fft_x;                      // contiguous scratch for the filter
+    DevBuf psi_alt, n_alt;             // second state plane for the fused RK4 iteration
     DevBuf partials, result;
     PinnedBuf host_result;
     cufftHandle plan = 0;
@@ -243,6 +245,7 @@ struct Engine final : EngineBase {
         if (const char* e = std::getenv("PHX_STAGE_SHAPE")) {
             const int v = std::atoi(e);
             if (v >= 0 && v < kShapes) shape = v;
+            if (v == kFusedShape && fused_eligible_static()) shape = v;
         }
         partials.alloc(sizeof(double) * 2 * std::max<long long>(max_blocks, 1024), stream);
         result.alloc(sizeof(double) * 4, stream);
@@ -254,10 +257,19 @@ struct Engine final : EngineBase {
     }
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
-    int cur_shape() const { return shape >= 0 ? shape : tune_step % kShapes; }
+    static constexpr int kFusedShape = kShapes;  // launch shape 4: whole RK4 iteration in one kernel
+    int n_candidates() const { return fused_eligible_static() ? kShapes + 1 : kShapes; }
+    int cur_shape() const { return shape >= 0 ? shape : tune_step % n_candidates(); }
+    // the fused iteration handles scalar RK4 with at most one pump and one
+    // potential group and no pulse (real temporal coefficients are checked
+    // every iteration)
+    bool fused_eligible_static() const {
+        return P.iterator == PHX_ITER_RK4 && !P.tetm && P.n_pump_groups <= 1 && P.n_potential_groups <= 1 &&
+               P.n_pulse_groups == 0;
+    }
     long long rows_per_block(int sh) const { return (long long)kShapeRB[sh] * kShapeWarps[sh]; }
     long long grid_y(long long r0, long long r1) const {
-        const long long rpb = rows_per_block(cur_shape());
+        const long long rpb = rows_per_block(cur_shape() == kFusedShape ? kDefaultShape : cur_shape());
         return (r1 - r0 + rpb - 1) / rpb;
     }
 
@@ -342,10 +354,16 @@ struct Engine final : EngineBase {
         const size_t esz = f.complex ? sizeof(C) : sizeof(T);
         char* dst = reinterpret_cast<char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
         PHX_CUDA(cudaMemcpy2DAsync(dst, esz * pitch, tmp.data(), esz * N_c, esz * N_c, N_r, cudaMemcpyHostToDevice, stream));
-        if (field == PHX_PSI_PLUS || field == PHX_PSI_MINUS) {
-            ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(*f.buf), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
-            PHX_CUDA(cudaGetLastError());
-        }
+        // ring of the uploaded plane: zeros along zero axes, periodic images
+        // along periodic axes (synchronize_halos after every upload,
+        // solver_initialization.cu:81-146)
+        if (f.complex)
+            ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(*f.buf, f.plane_index), N_r, N_c, pitch, G, P.periodic_x,
+                                                        P.periodic_y);
+        else
+            ring_fill_kernel<T><<<64, 256, 0, stream>>>(rplane(*f.buf, f.plane_index), N_r, N_c, pitch, G, P.periodic_x,
+                                                        P.periodic_y);
+        PHX_CUDA(cudaGetLastError());
         PHX_CUDA(cudaStreamSynchronize(stream));
     }
 
@@ -502,7 +520,7 @@ struct Engine final : EngineBase {
         dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
         cudaEvent_t a = nullptr;
         prof_begin(a);
-        switch (cur_shape()) {
+        switch (cur_shape() == kFusedShape ? kDefaultShape : cur_shape()) {
             case 0: go_scalar<KIND, RES, 0>(S, grid); break;
             case 1: go_scalar<KIND, RES, 1>(S, grid); break;
             case 2: go_scalar<KIND, RES, 2>(S, grid); break;
@@ -538,7 +556,7 @@ struct Engine final : EngineBase {
             dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
             cudaEvent_t a = nullptr;
             prof_begin(a);
-            switch (cur_shape()) {
+            switch (cur_shape() == kFusedShape ? kDefaultShape : cur_shape()) {
                 case 0: go_tetm<KIND, 0>(Q, grid); break;
                 case 1: go_tetm<KIND, 1>(Q, grid); break;
                 case 2: go_tetm<KIND, 2>(Q, grid); break;
@@ -555,7 +573,77 @@ struct Engine final : EngineBase {
     }
 
     // ------------------------------------------------------------ RK4
+    // Whole iteration in one launch (phx_step_fused.cuh).  Returns false when
+    // this iteration needs the per-stage kernels (complex temporal
+    // coefficients).
+    template <bool RES>
+    void go_fused(const FusedParams<T>& F) {
+        constexpr int TW = 32, TH = sizeof(T) == 4 ? 32 : 16, NT = 256;
+        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+        rk4_fused_kernel<T, RES, TW, TH, NT><<<grid, NT, 0, stream>>>(F);
+    }
+    bool step_rk4_fused() {
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
+        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
+        FusedParams<T> F;
+        std::memset(&F, 0, sizeof(F));
+        for (int s = 0; s < 4; ++s) {
+            if (P.n_pump_groups) {
+                const auto c = interp<T>(amp_pump[0], next_pump[0], cw[s]);
+                if (c.imag() != (T)0) return false;
+                F.pump_c[s] = c.real();
+            }
+            if (P.n_potential_groups) {
+                const auto c = interp<T>(amp_pot[0], next_pot[0], cw[s]);
+                if (c.imag() != (T)0) return false;
+                F.pot_c[s] = c.real();
+            }
+            F.b[s] = bw[s];
+            if (s < 3) F.dtw[s] = dt * aw[s];
+        }
+        if (!psi_alt.p) {
+            psi_alt.alloc(sizeof(C) * plane, stream);
+            n_alt.alloc(sizeof(T) * plane, stream);
+        }
+        F.N_r = N_r;
+        F.N_c = N_c;
+        F.img_x = P.periodic_x;
+        F.img_y = P.periodic_y;
+        F.pitch = pitch;
+        F.psi0 = cplane(psi[0]);
+        F.n0 = rplane(nres[0]);
+        F.psi1 = cplane(psi_alt);
+        F.n1 = rplane(n_alt);
+        F.pump = P.n_pump_groups ? rplane(pump[0]) : nullptr;
+        F.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
+        F.m2 = d.m2, F.odx2 = d.odx2, F.ody2 = d.ody2, F.meff = d.meff, F.ohb = d.ohb;
+        F.ohb_gc = d.ohb * (T)P.g_c;
+        F.half_gamma_c = (T)0.5 * (T)P.gamma_c;
+        F.ohb_gr = d.ohb * (T)P.g_r;
+        F.half_R = (T)0.5 * (T)P.R;
+        F.gamma_r = (T)P.gamma_r;
+        F.R = (T)P.R;
+        F.dt = dt;
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        if (P.use_reservoir)
+            go_fused<true>(F);
+        else
+            go_fused<false>(F);
+        const double pts = (double)N_r * N_c;
+        const double st = sizeof(C) + (P.use_reservoir ? sizeof(T) : 0);
+        prof_end(PHX_KERNEL_RK4_FUSED, a,
+                 pts * (2 * st + (P.n_pump_groups ? sizeof(T) : 0) + (P.n_potential_groups ? sizeof(T) : 0)));
+        ++launches;
+        PHX_CUDA(cudaGetLastError());
+        std::swap(psi[0].p, psi_alt.p);
+        std::swap(nres[0].p, n_alt.p);
+        return true;
+    }
+
     void step_rk4() {
+        if (cur_shape() == kFusedShape && step_rk4_fused()) return;
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
         const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
         const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
@@ -858,13 +946,13 @@ struct Engine final : EngineBase {
     void tune_record(cudaEvent_t ta, cudaEvent_t tb) {
         tb = get_event();
         PHX_CUDA(cudaEventRecord(tb, stream));
-        tune_ev[tune_step % kShapes].push_back({ta, tb});
+        tune_ev[tune_step % n_candidates()].push_back({ta, tb});
         ++tune_step;
-        if (tune_step < 2 * kShapes) return;
+        if (tune_step < 2 * n_candidates()) return;
         PHX_CUDA(cudaStreamSynchronize(stream));
         float best = 1e30f;
         int best_sh = kDefaultShape;
-        for (int sh = 0; sh < kShapes; ++sh) {
+        for (int sh = 0; sh < n_candidates(); ++sh) {
             float ms = 1e30f;
             for (size_t i = 1; i < tune_ev[sh].size(); ++i) {
                 float m = 0.f;

@@ -168,13 +168,20 @@ __device__ __forceinline__ void rhs_scalar(const StageParams<T>& P, long long id
     k_wf = wf;
 }
 
-template <typename T>
-__device__ __forceinline__ void write_images(const StageParams<T>& P, cx<T>* base, int r, int c, cx<T> v) {
-    const bool ex = P.img_x && (c == 0 || c == P.N_c - 1);
-    const bool ey = P.img_y && (r == 0 || r == P.N_r - 1);
+// Periodic images of a produced point (wavefunction and reservoir): every
+// point within kImgDepth of a periodic border is also written into the ring
+// on the opposite side, so the ring always holds images kImgDepth deep (the
+// fused iteration evaluates stage values on a 3-4 cell halo read straight
+// from the ring, as the reference does on its halo-padded subgrids).
+constexpr int kImgDepth = 4;
+template <typename T, typename V>
+__device__ __forceinline__ void write_images(const StageParams<T>& P, V* base, int r, int c, V v) {
+    const bool lx = P.img_x && c >= 0 && c < kImgDepth, hx = P.img_x && c >= P.N_c - kImgDepth && c < P.N_c;
+    const bool ly = P.img_y && r >= 0 && r < kImgDepth, hy = P.img_y && r >= P.N_r - kImgDepth && r < P.N_r;
+    const bool ex = lx || hx, ey = ly || hy;
     if (!(ex || ey)) return;
-    const int ci = c == 0 ? P.N_c : -1;
-    const int ri = r == 0 ? P.N_r : -1;
+    const int ci = lx ? c + P.N_c : c - P.N_c;
+    const int ri = ly ? r + P.N_r : r - P.N_r;
     if (ex) base[(long long)r * P.pitch + ci] = v;
     if (ey) base[(long long)ri * P.pitch + c] = v;
     if (ex && ey) base[(long long)ri * P.pitch + ci] = v;
@@ -349,7 +356,10 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
                     if constexpr (RES) str(P.n_out + idx, out_rv);
                     if (P.img_x | P.img_y) {
 #pragma unroll
-                        for (int j = 0; j < CPT; ++j) write_images(P, P.psi_out, r, c + j, out_wf.v[j]);
+                        for (int j = 0; j < CPT; ++j) {
+                            write_images(P, P.psi_out, r, c + j, out_wf.v[j]);
+                            if constexpr (RES) write_images(P, P.n_out, r, c + j, out_rv.v[j]);
+                        }
                     }
                 }
             }

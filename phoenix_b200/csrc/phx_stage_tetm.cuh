@@ -296,6 +296,8 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                         for (int j = 0; j < CPT; ++j) {
                             write_images(P, P.psi_out, r, c + j, owp.v[j]);
                             write_images(P, Q.psi_out, r, c + j, owm.v[j]);
+                            write_images(P, P.n_out, r, c + j, orp.v[j]);
+                            write_images(P, Q.n_out, r, c + j, orm.v[j]);
                         }
                     }
                 }

@@ -1,0 +1,183 @@
+// One launch per RK4 iteration: all four stages of RungeKutta4::step
+// (source/cuda_solver/solver/iterator/runge_kutta.cu:74-94) fused on an
+// on-chip tile.
+//
+// The reference evaluates a step on subgrids padded by a halo as wide as the
+// number of stages and lets every stage shrink the evaluated region by one
+// cell (GENERATE_SUBGRID_INDEX / CALCULATE_K, include/cuda/cuda_macro.cuh:43-49,
+// 110-134).  This kernel does the same with a TW x TH output tile: the state
+// is read once over the tile plus a 4-cell halo into shared memory, stage s
+// is evaluated over the tile plus (4 - s) cells, the stencil input of each
+// stage lives in shared memory (two ping-pong buffers) and the pointwise
+// values (y0, n, accumulator, pump, potential) stay in registers of the
+// thread that owns the point.  Every point is computed with the same
+// operations, in the same order, as by the per-stage kernels, so the result
+// is bit-identical to them and to the reference CPU build; HBM traffic per
+// point drops from the 236 B of four stage passes (FP32) to the compulsory
+// 32 B (read psi, n, pump, potential; write psi, n).
+//
+// The halo is read straight from the padded planes: along periodic axes the
+// rings of psi, n, pump and potential hold periodic images at least 4 deep
+// (uploads fill them; this kernel and the stage kernels write them for the
+// state they produce), along zero axes they hold zeros, which is exactly the
+// reference's halo after synchronize_halos (kernel_halo.cuh:50-76; pump and
+// potential halos are synchronised once at initialisation,
+// solver_initialization.cu:105-146).
+#pragma once
+
+#include "phx_device.cuh"
+#include "phx_stage.cuh"
+
+namespace phx {
+
+template <typename T>
+struct FusedParams {
+    int N_r, N_c;
+    int img_x, img_y;  // periodic axes: write images of outputs within kImg of a border
+    long long pitch;
+    const cx<T>* psi0;  // state in  (interior origin, padded plane)
+    const T* n0;
+    cx<T>* psi1;        // state out (a different plane)
+    T* n1;
+    const T* pump;      // one plane or nullptr
+    const T* pot;       // one plane or nullptr
+    T pump_c[4];        // real temporal coefficient of stage s
+    T pot_c[4];
+    T m2, odx2, ody2, meff, ohb;
+    T ohb_gc, half_gamma_c, ohb_gr, half_R, gamma_r, R;
+    T b[4];
+    T dtw[3];
+    T dt;
+};
+
+constexpr int kImg = kImgDepth;
+
+// gp_scalar right-hand side with real temporal coefficients (the common case
+// of constant / cos / gauss envelopes); identical to rhs_scalar<T, RES> for
+// pump_c / pot_c with zero imaginary parts.
+template <typename T, bool RES>
+__device__ __forceinline__ void rhs_fused(const FusedParams<T>& P, int s, cx<T> in_wf, cx<T> up, cx<T> dn, cx<T> left,
+                                          cx<T> right, T in_rv, T pump, T pot, bool has_pump, bool has_pot, cx<T>& k_wf,
+                                          T& k_rv) {
+    const cx<T> in_wf_mi = mi(in_wf);
+    const T in_psi_norm = abs2(in_wf);
+    cx<T> wf = smul(P.meff, cadd(cadd(smul(P.m2, in_wf), smul(P.ody2, cadd(dn, up))), smul(P.odx2, cadd(right, left))));
+    wf = smul(P.ohb, mi(wf));
+    wf = cadd(wf, smul(rmul(P.ohb_gc, in_psi_norm), in_wf_mi));
+    wf = csub(wf, smul(P.half_gamma_c, in_wf));
+    if constexpr (RES) {
+        const cx<T> rv = mk(in_rv, (T)0);
+        wf = cadd(wf, cmul(smul(P.ohb_gr, rv), in_wf_mi));
+        wf = cadd(wf, cmul(smul(P.half_R, rv), in_wf));
+        T krv = rmul(-radd(P.gamma_r, rmul(P.R, in_psi_norm)), in_rv);
+        if (has_pump) krv = radd(krv, rmul(pump, P.pump_c[s]));
+        k_rv = krv;
+    }
+    if (has_pot) {
+        const cx<T> potc = mk(rmul(pot, P.pot_c[s]), rmul(pot, (T)0));
+        wf = cadd(wf, cmul(smul(P.ohb, potc), in_wf_mi));
+    }
+    k_wf = wf;
+}
+
+template <typename T, typename V>
+__device__ __forceinline__ void fused_images(const FusedParams<T>& P, V* base, int r, int c, V v) {
+    const bool lx = P.img_x && c < kImg, hx = P.img_x && c >= P.N_c - kImg;
+    const bool ly = P.img_y && r < kImg, hy = P.img_y && r >= P.N_r - kImg;
+    if (!(lx || hx || ly || hy)) return;
+    const int cs = lx ? c + P.N_c : c - P.N_c;
+    const int rs = ly ? r + P.N_r : r - P.N_r;
+    if (lx || hx) base[(long long)r * P.pitch + cs] = v;
+    if (ly || hy) base[(long long)rs * P.pitch + c] = v;
+    if ((lx || hx) && (ly || hy)) base[(long long)rs * P.pitch + cs] = v;
+}
+
+// Block: NT threads, one TW x TH output tile.  Grid: (ceil(N_c/TW), ceil(N_r/TH)).
+template <typename T, bool RES, int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ FusedParams<T> P) {
+    constexpr int W4 = TW + 8, H4 = TH + 8;    // tile + 4-cell halo (stage-1 stencil input)
+    constexpr int W3 = TW + 6, H3 = TH + 6;    // tile + 3 (points of stage 1)
+    constexpr int NC = W3 * H3;
+    constexpr int OWN = (NC + NT - 1) / NT;    // points owned by a thread
+    __shared__ cx<T> sA[H4 * W4];
+    __shared__ cx<T> sB[H4 * W4];
+    const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
+    const long long pitch = P.pitch;
+    const bool has_pump = P.pump != nullptr, has_pot = P.pot != nullptr;
+    // rows / columns that may be addressed: [-kRing, N + kRing)
+    const int rmax = P.N_r + kRing - 1, cmax = P.N_c + kRing - 1;
+
+    // 1) psi0 over tile + 4 into sA (16-byte loads of two points where aligned)
+    for (int i = threadIdx.x; i < H4 * W4; i += NT) {
+        const int ry = i / W4, rx = i - ry * W4;
+        const int gy = min(ty0 - 4 + ry, rmax), gx = min(tx0 - 4 + rx, cmax);
+        sA[i] = P.psi0[(long long)gy * pitch + gx];
+    }
+    // 2) pointwise values of the owned points of tile + 3
+    cx<T> y0[OWN], acc[OWN];
+    T n0[OWN], ns[OWN], an[OWN], pu[OWN], po[OWN];
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        const int q = threadIdx.x + NT * j;
+        const int qy = q / W3, qx = q - qy * W3;
+        const int gy = min(ty0 - 3 + qy, rmax), gx = min(tx0 - 3 + qx, cmax);
+        const long long g = (long long)gy * pitch + gx;
+        n0[j] = (RES && q < NC) ? __ldg(P.n0 + g) : (T)0;
+        pu[j] = (RES && has_pump && q < NC) ? __ldg(P.pump + g) : (T)0;
+        po[j] = (has_pot && q < NC) ? __ldg(P.pot + g) : (T)0;
+        ns[j] = n0[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        const int q = threadIdx.x + NT * j;
+        const int qy = q / W3, qx = q - qy * W3;
+        y0[j] = q < NC ? sA[(qy + 1) * W4 + qx + 1] : mk((T)0, (T)0);
+    }
+
+    // 3) stages; stage s (0-based) covers R3 coordinates [s, W3 - s) x [s, H3 - s)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const cx<T>* in = (s & 1) ? sB : sA;
+        cx<T>* out = (s & 1) ? sA : sB;
+#pragma unroll
+        for (int j = 0; j < OWN; ++j) {
+            const int q = threadIdx.x + NT * j;
+            const int qy = q / W3, qx = q - qy * W3;
+            if (q >= NC || qy < s || qy >= H3 - s || qx < s || qx >= W3 - s) continue;
+            const int c4 = (qy + 1) * W4 + qx + 1;
+            const cx<T> ce = s == 0 ? y0[j] : in[c4];
+            cx<T> kw;
+            T kr = (T)0;
+            rhs_fused<T, RES>(P, s, ce, in[c4 - W4], in[c4 + W4], in[c4 - 1], in[c4 + 1], ns[j], pu[j], po[j], has_pump,
+                              has_pot, kw, kr);
+            if (s == 0) {
+                acc[j] = smul(P.b[0], kw);
+                an[j] = rmul(P.b[0], kr);
+            } else if (s < 3) {
+                acc[j] = cadd(acc[j], smul(P.b[s], kw));
+                an[j] = radd(an[j], rmul(P.b[s], kr));
+            }
+            if (s < 3) {
+                out[c4] = cadd(y0[j], smul(P.dtw[s], kw));
+                if constexpr (RES) ns[j] = radd(n0[j], rmul(P.dtw[s], kr));
+            } else {
+                const cx<T> ynew = cadd(y0[j], smul(P.dt, cadd(acc[j], smul(P.b[3], kw))));
+                const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx;
+                if (gy < P.N_r && gx < P.N_c) {
+                    const long long g = (long long)gy * pitch + gx;
+                    P.psi1[g] = ynew;
+                    if (P.img_x | P.img_y) fused_images(P, P.psi1, gy, gx, ynew);
+                    if constexpr (RES) {
+                        const T nnew = radd(n0[j], rmul(P.dt, radd(an[j], rmul(P.b[3], kr))));
+                        P.n1[g] = nnew;
+                        if (P.img_x | P.img_y) fused_images(P, P.n1, gy, gx, nnew);
+                    }
+                }
+            }
+        }
+        if (s < 3) __syncthreads();
+    }
+}
+
+}  // namespace phx
