@@ -197,11 +197,30 @@ PHX_API phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_m
 /* The handle's cudaStream_t, as void*. */
 PHX_API phx_status phx_get_stream(phx_handle* h, void** stream);
 
-/* Message of the last failed call on this handle (or of the last failed
- * phx_create in this thread when h is NULL). */
+/* Message of the last failed call on this handle (or, when h is NULL, of
+ * the last failed call in this thread that takes no handle: phx_create,
+ * phx_sum_abs2_noalloc). */
 PHX_API const char* phx_last_error(const phx_handle* h);
 
 PHX_API const char* phx_status_string(int32_t status);
+
+/* No counterpart in the reference.  FP64 sum of |z|^2 (complex field) or
+ * x^2 (real field) over an N_r x N_c device field with the given row pitch
+ * (elements), written to *out_dev (device memory), queued on `stream`
+ * (a cudaStream_t; NULL for the legacy default stream).  It allocates
+ * nothing, for callers that cannot call cudaMalloc: code running while
+ * another runtime captures a CUDA graph, hosts whose device memory belongs
+ * to their own allocator or pool, and loops that cannot take the device
+ * synchronisation of cudaMalloc / cudaFree.  Its scratch (the per-block
+ * partial sums) is a fixed 32 KiB array inside the library that every GPU
+ * loading the library keeps until exit, so fields are limited to
+ * 16,777,216 points (4096 x 4096); larger ones return PHX_ERR_INVALID_ARG.
+ * The first call on a device looks up that array's device address (with
+ * the device current); make that first call before any stream capture.
+ * All calls share the array: calls whose kernels overlap on the GPU race.
+ * Errors: phx_last_error(NULL). */
+PHX_API phx_status phx_sum_abs2_noalloc(const void* field_dev, int32_t dtype, int32_t is_complex, int32_t N_r,
+                                        int32_t N_c, int64_t row_pitch_elems, double* out_dev, void* stream);
 
 /* ABI version and build description ("sm_100a ..."). */
 PHX_API int32_t phx_abi_version(void);

@@ -75,6 +75,8 @@ _SIGS = {
     "phx_profile_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_double)]),
     "phx_last_error": (C.c_char_p, [C.c_void_p]),
+    "phx_sum_abs2_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                                       C.c_void_p, C.c_void_p]),
     "phx_status_string": (C.c_char_p, [C.c_int32]),
     "phx_abi_version": (C.c_int32, []),
     "phx_build_info": (C.c_char_p, []),

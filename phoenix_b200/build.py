@@ -39,7 +39,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if not force and up_to_date():
         return LIB
     cmd = [NVCC] + ARCH_FLAGS + CFLAGS + ["-shared", "-o", LIB + ".tmp", os.path.join(CSRC, "phx_runtime.cu"),
-                                          "-lcufft"]
+                                          os.path.join(CSRC, "phx_noalloc.cu"), "-lcufft"]
     if ptxas_info:
         cmd.insert(1, "-Xptxas=-v")
     if verbose:
