@@ -13,8 +13,9 @@ Legs of the JSON line:
   value      device time per iteration (CUDA events on the solver's stream),
              L2 flushed (256 MiB write) between timed iterations, max over ranks
   e2e        the same workload through the public API with host buffers:
-             upload psi0/n0, run in chunks of 100 iterations reading the FP64
-             norm back after each chunk, download psi and n at the end
+             upload psi0/n0 from pinned host memory, run in chunks of 100
+             iterations reading the FP64 norm back after each chunk, download
+             psi and n into pinned host memory at the end
   roofline   the dominant kernel (fused RK4 stage 2/3) from per-launch CUDA
              events recorded by the library on its stream during the timed
              region: algorithmic bytes / average duration vs measured HBM peak
@@ -56,6 +57,9 @@ MASK_EVERY = 100
 P_TH = 0.15 * 0.225 / 0.01
 METRIC = "us_per_rk4_iteration_1024x1024"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+KERNEL_NAMES = {"rk4_fused": "rk4_fused_kernel / rk4_tma_kernel (whole RK4 iteration)",
+                "rk4_mid": "stage_scalar_kernel<kRk4Mid>", "rk4_first": "stage_scalar_kernel<kRk4First>",
+                "rk4_last": "stage_scalar_kernel<kRk4Last>"}
 
 
 def workload(n, seed=2):
@@ -316,7 +320,12 @@ def main():
     # end to end through the public API, host buffers in and out
     e2e_iters = args.steps
     chunk = 100
-    pinned_psi = torch.from_numpy(np.ascontiguousarray(wl["psi0"])).pin_memory().numpy()
+    cdt = torch.complex64 if args.dtype == "f32" else torch.complex128
+    rdt = torch.float32 if args.dtype == "f32" else torch.float64
+    pinned_psi = torch.from_numpy(np.ascontiguousarray(wl["psi0"])).to(cdt).pin_memory().numpy()
+    pinned_n = torch.zeros((n, n), dtype=rdt).pin_memory().numpy()
+    pinned_psi_out = torch.empty((n, n), dtype=cdt).pin_memory().numpy()
+    pinned_n_out = torch.empty((n, n), dtype=rdt).pin_memory().numpy()
     barrier()
     torch.cuda.synchronize()
     s2 = pb.Solver(sp)
@@ -329,7 +338,7 @@ def main():
     with torch.cuda.stream(st2):
         a0.record(st2)
     s2.set_field("psi_plus", pinned_psi)
-    s2.set_field("n_plus", np.zeros((n, n)))
+    s2.set_field("n_plus", pinned_n)
     done = 0
     norms = []
     while done < e2e_iters:
@@ -337,8 +346,8 @@ def main():
         s2.run(k)
         norms.append(s2.sum_abs2("psi_plus"))
         done += k
-    psi_out = s2.get_field("psi_plus")
-    n_out = s2.get_field("n_plus")
+    psi_out = s2.get_field("psi_plus", out=pinned_psi_out)
+    n_out = s2.get_field("n_plus", out=pinned_n_out)
     with torch.cuda.stream(st2):
         a1.record(st2)
     torch.cuda.synchronize()
@@ -349,8 +358,8 @@ def main():
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
     e2e_ms = float(t_e2e.item())
     esz = 4 if args.dtype == "f32" else 8
-    h2d = n * n * (2 * 8 + 8)  # psi0 (complex) and n0 from FP64 host arrays
-    d2h = n * n * (2 * 8 + 8) + 16 * ((e2e_iters + chunk - 1) // chunk)
+    h2d = n * n * 3 * esz  # psi0 (complex) and n0, pinned, in the build precision
+    d2h = n * n * 3 * esz + 8 * ((e2e_iters + chunk - 1) // chunk)  # psi, n and one FP64 norm per chunk
     assert np.isfinite(psi_out).all() and np.isfinite(n_out).all() and all(np.isfinite(norms))
 
     # roofline of the dominant kernel (fused RK4 middle stage)
@@ -360,17 +369,22 @@ def main():
         with open(peaks_path) as f:
             peak = float(json.load(f)["hbm_gbs"])
         peak_src = "measured"
-    dom = prof.get("rk4_mid", {"ms": float("nan"), "launches": 1, "bytes": float("nan")})
+    # dominant kernel: the family with the largest device time in the timed region
+    dom_name = max((k for k in prof if k != "other"), key=lambda k: prof[k]["ms"])
+    dom = prof[dom_name]
     per_launch_bytes = dom["bytes"] / dom["launches"]
     per_launch_ms = dom["ms"] / dom["launches"]
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "rk4_mid_stage_traffic.json")
+    # DRAM traffic per launch from the committed ncu summary of that kernel at
+    # 4096^2 (the largest case ncu captures here), scaled to this grid by points
+    tfile = os.path.join(ROOT, "profiles", "traffic_per_point.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
             tj = json.load(f)
-        if tj.get("dtype") == args.dtype and tj.get("n") == n:
-            traffic = tj.get("bytes_per_launch")
+        key = f"{dom_name}_{args.dtype}"
+        if key in tj:
+            traffic = tj[key]["bytes_per_point"] * n * n
     step_bytes = sum(v["bytes"] for k, v in prof.items() if k.startswith("rk4")) / args.steps
     kernels_ms = {k: v["ms"] / v["launches"] for k, v in prof.items()}
 
@@ -396,7 +410,7 @@ def main():
                 "e2e": {"value": e2e_ms * 1e3, "unit": "us/iter", "h2d_bytes_per_step": h2d / e2e_iters,
                         "d2h_bytes_per_step": d2h / e2e_iters},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "kernel": "stage_scalar_kernel<rk4_mid>",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": KERNEL_NAMES.get(dom_name, dom_name),
                              "peak_source": peak_src, "bytes_per_launch": per_launch_bytes,
                              "step_alg_bytes": step_bytes,
                              "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},

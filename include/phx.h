@@ -117,8 +117,9 @@ typedef struct {
     int64_t accepted, rejected;     /* DP45 attempts */
     int64_t fft_filters;            /* k-space mask applications */
     int64_t kernel_launches;        /* this library's kernels launched */
-    int32_t launch_shape;           /* launch shape in use: 0-3 per-stage kernels, 4 fused RK4
-                                       iteration, -1 while the first iterations time them */
+    int32_t launch_shape;           /* launch shape in use: 0-3 per-stage kernels, 4-7 the fused
+                                       RK4 iteration (tile shapes), -1 while the first iterations
+                                       time them */
     int32_t reserved;
 } phx_step_info;
 

@@ -28,6 +28,7 @@
 #include "phx_stage.cuh"
 #include "phx_stage_tetm.cuh"
 #include "phx_step_fused.cuh"
+#include "phx_step_tma.cuh"
 
 namespace phx {
 
@@ -165,7 +166,7 @@ struct Engine final : EngineBase {
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 1];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 5];
     static constexpr int kRingBlocks = 64;
     using C = cx<T>;
 
@@ -184,6 +185,7 @@ struct Engine final : EngineBase {
     DevBuf mask[2];                    // fft-shifted mask, contiguous N_r*N_c
     DevBuf fft_x;                      // contiguous scratch for the filter
     DevBuf psi_alt, n_alt;             // second state plane for the fused RK4 iteration
+    DevBuf err_flag;                   // set by kernels whose bounded waits gave up
     DevBuf partials, result;
     PinnedBuf host_result;
     cufftHandle plan = 0;
@@ -245,7 +247,7 @@ struct Engine final : EngineBase {
         if (const char* e = std::getenv("PHX_STAGE_SHAPE")) {
             const int v = std::atoi(e);
             if (v >= 0 && v < kShapes) shape = v;
-            if (v == kFusedShape && fused_eligible_static()) shape = v;
+            if (v >= kFusedShape && v < kFusedShape + kFusedShapes && fused_eligible_static()) shape = v;
         }
         partials.alloc(sizeof(double) * 2 * std::max<long long>(max_blocks, 1024), stream);
         result.alloc(sizeof(double) * 4, stream);
@@ -257,8 +259,10 @@ struct Engine final : EngineBase {
     }
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
-    static constexpr int kFusedShape = kShapes;  // launch shape 4: whole RK4 iteration in one kernel
-    int n_candidates() const { return fused_eligible_static() ? kShapes + 1 : kShapes; }
+    static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
+    static constexpr int kFusedShapes = 5;  // shape 8: persistent TMA-fed variant
+    int n_candidates() const { return fused_eligible_static() ? kShapes + kFusedShapes : kShapes; }
+    bool is_fused(int sh) const { return sh >= kFusedShape; }
     int cur_shape() const { return shape >= 0 ? shape : tune_step % n_candidates(); }
     // the fused iteration handles scalar RK4 with at most one pump and one
     // potential group and no pulse (real temporal coefficients are checked
@@ -269,7 +273,7 @@ struct Engine final : EngineBase {
     }
     long long rows_per_block(int sh) const { return (long long)kShapeRB[sh] * kShapeWarps[sh]; }
     long long grid_y(long long r0, long long r1) const {
-        const long long rpb = rows_per_block(cur_shape() == kFusedShape ? kDefaultShape : cur_shape());
+        const long long rpb = rows_per_block(is_fused(cur_shape()) ? kDefaultShape : cur_shape());
         return (r1 - r0 + rpb - 1) / rpb;
     }
 
@@ -349,11 +353,17 @@ struct Engine final : EngineBase {
         FieldRef f = field_ref(field, group);
         const long long want = f.complex ? 2 * N : N;
         if (count != want) fail(PHX_ERR_INVALID_ARG, "expected " + std::to_string(want) + " values, got " + std::to_string(count));
+        // same precision: copy straight from the caller's buffer (DMA when it is
+        // pinned); otherwise convert through a host staging vector
         std::vector<T> tmp;
-        convert_in(host, dtype, (size_t)want, tmp);
+        const void* src = host;
+        if ((dtype == PHX_F64) != (sizeof(T) == 8)) {
+            convert_in(host, dtype, (size_t)want, tmp);
+            src = tmp.data();
+        }
         const size_t esz = f.complex ? sizeof(C) : sizeof(T);
         char* dst = reinterpret_cast<char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
-        PHX_CUDA(cudaMemcpy2DAsync(dst, esz * pitch, tmp.data(), esz * N_c, esz * N_c, N_r, cudaMemcpyHostToDevice, stream));
+        PHX_CUDA(cudaMemcpy2DAsync(dst, esz * pitch, src, esz * N_c, esz * N_c, N_r, cudaMemcpyHostToDevice, stream));
         // ring of the uploaded plane: zeros along zero axes, periodic images
         // along periodic axes (synchronize_halos after every upload,
         // solver_initialization.cu:81-146)
@@ -369,15 +379,22 @@ struct Engine final : EngineBase {
 
     void get_field(int field, int group, void* host, int64_t count, int dtype) override {
         if (!host) fail(PHX_ERR_INVALID_ARG, "host pointer is NULL");
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        check_err_flag();
         if (dtype != PHX_F32 && dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "bad host dtype");
         if (field == PHX_FFT_MASK_PLUS || field == PHX_FFT_MASK_MINUS) fail(PHX_ERR_UNSUPPORTED, "mask read-back not provided");
         FieldRef f = field_ref(field, group);
         const long long N = (long long)N_r * N_c;
         const long long want = f.complex ? 2 * N : N;
         if (count != want) fail(PHX_ERR_INVALID_ARG, "expected " + std::to_string(want) + " values");
-        std::vector<T> tmp((size_t)want);
         const size_t esz = f.complex ? sizeof(C) : sizeof(T);
         const char* src = reinterpret_cast<const char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
+        if ((dtype == PHX_F64) == (sizeof(T) == 8)) {
+            PHX_CUDA(cudaMemcpy2DAsync(host, esz * N_c, src, esz * pitch, esz * N_c, N_r, cudaMemcpyDeviceToHost, stream));
+            PHX_CUDA(cudaStreamSynchronize(stream));
+            return;
+        }
+        std::vector<T> tmp((size_t)want);
         PHX_CUDA(cudaMemcpy2DAsync(tmp.data(), esz * N_c, src, esz * pitch, esz * N_c, N_r, cudaMemcpyDeviceToHost, stream));
         PHX_CUDA(cudaStreamSynchronize(stream));
         if (dtype == PHX_F64) {
@@ -520,7 +537,7 @@ struct Engine final : EngineBase {
         dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
         cudaEvent_t a = nullptr;
         prof_begin(a);
-        switch (cur_shape() == kFusedShape ? kDefaultShape : cur_shape()) {
+        switch (is_fused(cur_shape()) ? kDefaultShape : cur_shape()) {
             case 0: go_scalar<KIND, RES, 0>(S, grid); break;
             case 1: go_scalar<KIND, RES, 1>(S, grid); break;
             case 2: go_scalar<KIND, RES, 2>(S, grid); break;
@@ -556,7 +573,7 @@ struct Engine final : EngineBase {
             dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
             cudaEvent_t a = nullptr;
             prof_begin(a);
-            switch (cur_shape() == kFusedShape ? kDefaultShape : cur_shape()) {
+            switch (is_fused(cur_shape()) ? kDefaultShape : cur_shape()) {
                 case 0: go_tetm<KIND, 0>(Q, grid); break;
                 case 1: go_tetm<KIND, 1>(Q, grid); break;
                 case 2: go_tetm<KIND, 2>(Q, grid); break;
@@ -576,11 +593,93 @@ struct Engine final : EngineBase {
     // Whole iteration in one launch (phx_step_fused.cuh).  Returns false when
     // this iteration needs the per-stage kernels (complex temporal
     // coefficients).
-    template <bool RES>
-    void go_fused(const FusedParams<T>& F) {
-        constexpr int TW = 32, TH = sizeof(T) == 4 ? 32 : 16, NT = 256;
+    // fused-iteration tile shapes (TW x TH points, NT threads); FP64 uses half-height tiles
+    template <bool RES, int TW, int TH, int NT>
+    void go_fused_shape(const FusedParams<T>& F) {
         dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
         rk4_fused_kernel<T, RES, TW, TH, NT><<<grid, NT, 0, stream>>>(F);
+    }
+    // ---- TMA-fed persistent variant
+    using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    EncodeFn encode = nullptr;
+    int tma_blocks_per_sm = 0, sm_count = 0;
+    void tensor_map(CUtensorMap* m, void* alloc_base, bool complex, int box_w_points, int box_h) {
+        if (!encode) {
+            cudaDriverEntryPointQueryResult q;
+            void* fn = nullptr;
+            PHX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+            if (q != cudaDriverEntryPointSuccess || !fn) fail(PHX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+            encode = reinterpret_cast<EncodeFn>(fn);
+        }
+        const int per = complex ? 2 : 1;
+        const cuuint64_t dims[2] = {(cuuint64_t)(per * pitch), (cuuint64_t)rows};
+        const cuuint64_t strides[1] = {(cuuint64_t)(per * pitch * sizeof(T))};
+        const cuuint32_t box[2] = {(cuuint32_t)(per * box_w_points), (cuuint32_t)box_h};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = encode(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
+                                  alloc_base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) fail(PHX_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    }
+    template <bool RES, int TW, int TH, int NT>
+    void go_tma(const FusedParams<T>& F) {
+        using Lay = TmaLayout<T, TW, TH>;
+        static_assert(TW % 4 == 0, "TMA box x alignment needs tile origins on 16-byte boundaries");
+        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT>;
+        if (!tma_blocks_per_sm) {
+            PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
+            PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_blocks_per_sm, kern, NT, Lay::total));
+            PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
+            if (tma_blocks_per_sm < 1) fail(PHX_ERR_UNSUPPORTED, "TMA iteration kernel does not fit on an SM");
+        }
+        if (!err_flag.p) err_flag.alloc(sizeof(int), stream);
+        TmaParams<T> Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.f = F;
+        // tensor maps over whole allocations (padded (0,0) = interior (-G,-G))
+        tensor_map(&Q.psi_map, reinterpret_cast<char*>(cplane(psi[0])) - sizeof(C) * (G * pitch + G), true, TW + 8, TH + 8);
+        tensor_map(&Q.n_map, reinterpret_cast<char*>(rplane(nres[0])) - sizeof(T) * (G * pitch + G), false, TW + 8, TH + 6);
+        Q.has_pump = F.pump != nullptr;
+        Q.has_pot = F.pot != nullptr;
+        tensor_map(&Q.pump_map, pump[0].p, false, TW + 8, TH + 6);
+        tensor_map(&Q.pot_map, pot[0].p, false, TW + 8, TH + 6);
+        Q.tiles_x = (N_c + TW - 1) / TW;
+        Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
+        Q.err = static_cast<int*>(err_flag.p);
+        const int blocks = std::min(Q.n_tiles, tma_blocks_per_sm * sm_count);
+        kern<<<blocks, NT, Lay::total, stream>>>(Q);
+    }
+    void check_err_flag() {
+        if (!err_flag.p) return;
+        int v = 0;
+        PHX_CUDA(cudaMemcpy(&v, err_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (v) {
+            PHX_CUDA(cudaMemset(err_flag.p, 0, sizeof(int)));
+            fail(PHX_ERR_TIMEOUT, "a bounded wait for TMA data gave up; the iteration's results are invalid");
+        }
+    }
+
+    template <bool RES>
+    void go_fused(const FusedParams<T>& F) {
+        constexpr bool f32 = sizeof(T) == 4;
+        if (cur_shape() - kFusedShape == 4) {
+            go_tma<RES, 32, f32 ? 32 : 16, 256>(F);
+            return;
+        }
+        switch (cur_shape() - kFusedShape) {
+            case 0: go_fused_shape<RES, 32, f32 ? 32 : 16, 256>(F); break;
+            case 1: go_fused_shape<RES, 64, f32 ? 16 : 8, 256>(F); break;
+            case 2: go_fused_shape<RES, 32, f32 ? 16 : 8, 128>(F); break;
+            default:
+                if constexpr (f32)
+                    go_fused_shape<RES, 64, 32, 512>(F);
+                else
+                    go_fused_shape<RES, 32, 24, 384>(F);  // 48 KiB static shared-memory limit
+                break;
+        }
     }
     bool step_rk4_fused() {
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
@@ -643,7 +742,7 @@ struct Engine final : EngineBase {
     }
 
     void step_rk4() {
-        if (cur_shape() == kFusedShape && step_rk4_fused()) return;
+        if (is_fused(cur_shape()) && step_rk4_fused()) return;
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
         const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
         const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
@@ -970,6 +1069,8 @@ struct Engine final : EngineBase {
     }
 
     double sum_abs2(int field) override {
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        check_err_flag();
         FieldRef f = field_ref(field, 0);
         const int blocks = 296;
         if (f.complex)

@@ -52,9 +52,12 @@ struct FusedParams {
 
 constexpr int kImg = kImgDepth;
 
-// gp_scalar right-hand side with real temporal coefficients (the common case
-// of constant / cos / gauss envelopes); identical to rhs_scalar<T, RES> for
-// pump_c / pot_c with zero imaginary parts.
+// gp_scalar right-hand side with real temporal coefficients (constant / cos /
+// gauss envelopes) and the reservoir stored real.  The reference multiplies
+// complex numbers whose imaginary part is exactly zero here
+// ((g_r n) * (-i psi), (R/2 n) * psi, (V c) * (-i psi)); this keeps only the
+// products that are not with that zero, which changes no result except,
+// possibly, the sign of an exact zero.
 template <typename T, bool RES>
 __device__ __forceinline__ void rhs_fused(const FusedParams<T>& P, int s, cx<T> in_wf, cx<T> up, cx<T> dn, cx<T> left,
                                           cx<T> right, T in_rv, T pump, T pot, bool has_pump, bool has_pot, cx<T>& k_wf,
@@ -66,17 +69,13 @@ __device__ __forceinline__ void rhs_fused(const FusedParams<T>& P, int s, cx<T> 
     wf = cadd(wf, smul(rmul(P.ohb_gc, in_psi_norm), in_wf_mi));
     wf = csub(wf, smul(P.half_gamma_c, in_wf));
     if constexpr (RES) {
-        const cx<T> rv = mk(in_rv, (T)0);
-        wf = cadd(wf, cmul(smul(P.ohb_gr, rv), in_wf_mi));
-        wf = cadd(wf, cmul(smul(P.half_R, rv), in_wf));
+        wf = cadd(wf, smul(rmul(P.ohb_gr, in_rv), in_wf_mi));
+        wf = cadd(wf, smul(rmul(P.half_R, in_rv), in_wf));
         T krv = rmul(-radd(P.gamma_r, rmul(P.R, in_psi_norm)), in_rv);
         if (has_pump) krv = radd(krv, rmul(pump, P.pump_c[s]));
         k_rv = krv;
     }
-    if (has_pot) {
-        const cx<T> potc = mk(rmul(pot, P.pot_c[s]), rmul(pot, (T)0));
-        wf = cadd(wf, cmul(smul(P.ohb, potc), in_wf_mi));
-    }
+    if (has_pot) wf = cadd(wf, smul(rmul(P.ohb, rmul(pot, P.pot_c[s])), in_wf_mi));
     k_wf = wf;
 }
 
@@ -93,85 +92,114 @@ __device__ __forceinline__ void fused_images(const FusedParams<T>& P, V* base, i
 }
 
 // Block: NT threads, one TW x TH output tile.  Grid: (ceil(N_c/TW), ceil(N_r/TH)).
+// A thread owns horizontal pairs of points of tile + 3 (R3) for all four
+// stages: their y0, reservoir, accumulators, pump and potential stay in its
+// registers; the stencil input of each stage is in shared memory.  Shared
+// planes are stored with one leading pad column so that every pair starts on
+// a 16-byte boundary.
 template <typename T, bool RES, int TW, int TH, int NT>
 __global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ FusedParams<T> P) {
+    static_assert(TW % 2 == 0, "pairs");
     constexpr int W4 = TW + 8, H4 = TH + 8;    // tile + 4-cell halo (stage-1 stencil input)
+    constexpr int SW = W4 + 2;                 // shared row: pad + W4 + pad
     constexpr int W3 = TW + 6, H3 = TH + 6;    // tile + 3 (points of stage 1)
-    constexpr int NC = W3 * H3;
-    constexpr int OWN = (NC + NT - 1) / NT;    // points owned by a thread
-    __shared__ cx<T> sA[H4 * W4];
-    __shared__ cx<T> sB[H4 * W4];
+    constexpr int PW = W3 / 2;                 // pairs per R3 row
+    constexpr int NP = PW * H3;
+    constexpr int OWN = (NP + NT - 1) / NT;    // pairs owned by a thread
+    __shared__ __align__(16) cx<T> sA[H4 * SW];
+    __shared__ __align__(16) cx<T> sB[H4 * SW];
     const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
     const long long pitch = P.pitch;
     const bool has_pump = P.pump != nullptr, has_pot = P.pot != nullptr;
-    // rows / columns that may be addressed: [-kRing, N + kRing)
     const int rmax = P.N_r + kRing - 1, cmax = P.N_c + kRing - 1;
 
-    // 1) psi0 over tile + 4 into sA (16-byte loads of two points where aligned)
+    // 1) psi0 over tile + 4 into sA; R4 point (ry, rx) at sA[ry * SW + rx + 1]
     for (int i = threadIdx.x; i < H4 * W4; i += NT) {
         const int ry = i / W4, rx = i - ry * W4;
         const int gy = min(ty0 - 4 + ry, rmax), gx = min(tx0 - 4 + rx, cmax);
-        sA[i] = P.psi0[(long long)gy * pitch + gx];
+        sA[ry * SW + rx + 1] = P.psi0[(long long)gy * pitch + gx];
     }
-    // 2) pointwise values of the owned points of tile + 3
-    cx<T> y0[OWN], acc[OWN];
-    T n0[OWN], ns[OWN], an[OWN], pu[OWN], po[OWN];
+    // 2) pointwise values of the owned pairs; R3 pair (qy, qx..qx+1)
+    cx<T> y0[OWN][2], acc[OWN][2];
+    T n0[OWN][2], ns[OWN][2], an[OWN][2], pu[OWN][2], po[OWN][2];
 #pragma unroll
     for (int j = 0; j < OWN; ++j) {
-        const int q = threadIdx.x + NT * j;
-        const int qy = q / W3, qx = q - qy * W3;
-        const int gy = min(ty0 - 3 + qy, rmax), gx = min(tx0 - 3 + qx, cmax);
-        const long long g = (long long)gy * pitch + gx;
-        n0[j] = (RES && q < NC) ? __ldg(P.n0 + g) : (T)0;
-        pu[j] = (RES && has_pump && q < NC) ? __ldg(P.pump + g) : (T)0;
-        po[j] = (has_pot && q < NC) ? __ldg(P.pot + g) : (T)0;
-        ns[j] = n0[j];
+        const int p = threadIdx.x + NT * j;
+        const int qy = p / PW, qx = 2 * (p - qy * PW);
+        const bool own = p < NP;
+        const int gy = min(ty0 - 3 + qy, rmax);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int gx = min(tx0 - 3 + qx + h, cmax);
+            const long long g = (long long)gy * pitch + gx;
+            n0[j][h] = (RES && own) ? __ldg(P.n0 + g) : (T)0;
+            pu[j][h] = (RES && has_pump && own) ? __ldg(P.pump + g) : (T)0;
+            po[j][h] = (has_pot && own) ? __ldg(P.pot + g) : (T)0;
+            ns[j][h] = n0[j][h];
+        }
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < OWN; ++j) {
-        const int q = threadIdx.x + NT * j;
-        const int qy = q / W3, qx = q - qy * W3;
-        y0[j] = q < NC ? sA[(qy + 1) * W4 + qx + 1] : mk((T)0, (T)0);
+        const int p = threadIdx.x + NT * j;
+        const int qy = p / PW, qx = 2 * (p - qy * PW);
+        const int e = (qy + 1) * SW + qx + 2;  // shared index of the pair's first point
+        y0[j][0] = p < NP ? sA[e] : mk((T)0, (T)0);
+        y0[j][1] = p < NP ? sA[e + 1] : mk((T)0, (T)0);
     }
 
-    // 3) stages; stage s (0-based) covers R3 coordinates [s, W3 - s) x [s, H3 - s)
+    // 3) stages; stage s (0-based) covers R3 [s, H3 - s) x [s, W3 - s).  A pair
+    // straddling the x edge computes both points: the outer one is never read
+    // by a later stage nor stored.
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
         const cx<T>* in = (s & 1) ? sB : sA;
         cx<T>* out = (s & 1) ? sA : sB;
 #pragma unroll
         for (int j = 0; j < OWN; ++j) {
-            const int q = threadIdx.x + NT * j;
-            const int qy = q / W3, qx = q - qy * W3;
-            if (q >= NC || qy < s || qy >= H3 - s || qx < s || qx >= W3 - s) continue;
-            const int c4 = (qy + 1) * W4 + qx + 1;
-            const cx<T> ce = s == 0 ? y0[j] : in[c4];
-            cx<T> kw;
-            T kr = (T)0;
-            rhs_fused<T, RES>(P, s, ce, in[c4 - W4], in[c4 + W4], in[c4 - 1], in[c4 + 1], ns[j], pu[j], po[j], has_pump,
-                              has_pot, kw, kr);
+            const int p = threadIdx.x + NT * j;
+            const int qy = p / PW, qx = 2 * (p - qy * PW);
+            if (p >= NP || qy < s || qy >= H3 - s || qx + 1 < s || qx >= W3 - s) continue;
+            const int e = (qy + 1) * SW + qx + 2;
+            cx<T> c0, c1;
             if (s == 0) {
-                acc[j] = smul(P.b[0], kw);
-                an[j] = rmul(P.b[0], kr);
-            } else if (s < 3) {
-                acc[j] = cadd(acc[j], smul(P.b[s], kw));
-                an[j] = radd(an[j], rmul(P.b[s], kr));
-            }
-            if (s < 3) {
-                out[c4] = cadd(y0[j], smul(P.dtw[s], kw));
-                if constexpr (RES) ns[j] = radd(n0[j], rmul(P.dtw[s], kr));
+                c0 = y0[j][0];
+                c1 = y0[j][1];
             } else {
-                const cx<T> ynew = cadd(y0[j], smul(P.dt, cadd(acc[j], smul(P.b[3], kw))));
-                const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx;
-                if (gy < P.N_r && gx < P.N_c) {
-                    const long long g = (long long)gy * pitch + gx;
-                    P.psi1[g] = ynew;
-                    if (P.img_x | P.img_y) fused_images(P, P.psi1, gy, gx, ynew);
-                    if constexpr (RES) {
-                        const T nnew = radd(n0[j], rmul(P.dt, radd(an[j], rmul(P.b[3], kr))));
-                        P.n1[g] = nnew;
-                        if (P.img_x | P.img_y) fused_images(P, P.n1, gy, gx, nnew);
+                c0 = in[e];
+                c1 = in[e + 1];
+            }
+            const cx<T> u0 = in[e - SW], u1 = in[e - SW + 1];
+            const cx<T> d0 = in[e + SW], d1 = in[e + SW + 1];
+            const cx<T> lft = in[e - 1], rgt = in[e + 2];
+            cx<T> kw[2];
+            T kr[2] = {(T)0, (T)0};
+            rhs_fused<T, RES>(P, s, c0, u0, d0, lft, c1, ns[j][0], pu[j][0], po[j][0], has_pump, has_pot, kw[0], kr[0]);
+            rhs_fused<T, RES>(P, s, c1, u1, d1, c0, rgt, ns[j][1], pu[j][1], po[j][1], has_pump, has_pot, kw[1], kr[1]);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (s == 0) {
+                    acc[j][h] = smul(P.b[0], kw[h]);
+                    an[j][h] = rmul(P.b[0], kr[h]);
+                } else if (s < 3) {
+                    acc[j][h] = cadd(acc[j][h], smul(P.b[s], kw[h]));
+                    an[j][h] = radd(an[j][h], rmul(P.b[s], kr[h]));
+                }
+                if (s < 3) {
+                    out[e + h] = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
+                    if constexpr (RES) ns[j][h] = radd(n0[j][h], rmul(P.dtw[s], kr[h]));
+                } else {
+                    const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
+                    if (qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {
+                        const cx<T> ynew = cadd(y0[j][h], smul(P.dt, cadd(acc[j][h], smul(P.b[3], kw[h]))));
+                        const long long g = (long long)gy * pitch + gx;
+                        P.psi1[g] = ynew;
+                        if (P.img_x | P.img_y) fused_images(P, P.psi1, gy, gx, ynew);
+                        if constexpr (RES) {
+                            const T nnew = radd(n0[j][h], rmul(P.dt, radd(an[j][h], rmul(P.b[3], kr[h]))));
+                            P.n1[g] = nnew;
+                            if (P.img_x | P.img_y) fused_images(P, P.n1, gy, gx, nnew);
+                        }
                     }
                 }
             }

@@ -139,27 +139,39 @@ class Solver:
     def _shape(self):
         return int(self.system.N_r), int(self.system.N_c)
 
+    def _host_types(self):
+        f32 = self.system.dtype not in ("f64", "fp64", "double")
+        return (np.complex64, np.float32, L.F32) if f32 else (np.complex128, np.float64, L.F64)
+
     def set_field(self, name: str, values, group: int = 0):
+        """Upload a full N_r x N_c field.  Arrays already in the build precision
+        (complex64 / float32 for FP32) are copied without conversion; pinned
+        host memory then goes straight to the device by DMA."""
         fid = L.FIELDS[name]
         a = np.asarray(values)
         if a.shape != self._shape():
             raise ValueError(f"{name}: expected shape {self._shape()}, got {a.shape}")
+        ctype, rtype, code = self._host_types()
         if name in L.COMPLEX_FIELDS:
-            buf = np.ascontiguousarray(np.stack([a.real, a.imag], axis=-1).astype(np.float64))
+            buf = np.ascontiguousarray(a, dtype=ctype).view(rtype)
         else:
-            buf = np.ascontiguousarray(np.real(a).astype(np.float64))
-        L.check(self._lib.phx_set_field(self._h, fid, group, buf.ctypes.data_as(C.c_void_p), buf.size, L.F64), self._h)
+            buf = np.ascontiguousarray(np.real(a), dtype=rtype)
+        L.check(self._lib.phx_set_field(self._h, fid, group, buf.ctypes.data_as(C.c_void_p), buf.size, code), self._h)
 
-    def get_field(self, name: str, group: int = 0):
+    def get_field(self, name: str, group: int = 0, out=None):
+        """Download a field (complex64 / float32 for FP32 builds, complex128 /
+        float64 for FP64); `out` may be a preallocated array of that type."""
         fid = L.FIELDS[name]
         cplx = name in L.COMPLEX_FIELDS
-        n = self._shape()[0] * self._shape()[1] * (2 if cplx else 1)
-        buf = np.empty(n, dtype=np.float64)
-        L.check(self._lib.phx_get_field(self._h, fid, group, buf.ctypes.data_as(C.c_void_p), n, L.F64), self._h)
-        if cplx:
-            b = buf.reshape(self._shape() + (2,))
-            return b[..., 0] + 1j * b[..., 1]
-        return buf.reshape(self._shape())
+        ctype, rtype, code = self._host_types()
+        want = ctype if cplx else rtype
+        if out is None:
+            out = np.empty(self._shape(), dtype=want)
+        if out.shape != self._shape() or out.dtype != want or not out.flags.c_contiguous:
+            raise ValueError(f"{name}: out must be a C-contiguous {np.dtype(want).name} array of shape {self._shape()}")
+        view = out.view(rtype)
+        L.check(self._lib.phx_get_field(self._h, fid, group, view.ctypes.data_as(C.c_void_p), view.size, code), self._h)
+        return out
 
     # -- time
     @property

@@ -136,7 +136,7 @@ SHAPE_CASES = ["rk4_f64_zero", "rk4_f64_periodic", "rk4_f64_mixed_rect", "rk4_f3
                "rk4_f64_temporal", "rk4_f64_nores"]
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 @pytest.mark.parametrize("name", SHAPE_CASES)
 def test_every_launch_shape_gives_identical_results(require_gpu, shape, name, monkeypatch):
     """The autotuner may pick any launch shape (0-3: one kernel per RK stage,
@@ -147,7 +147,8 @@ def test_every_launch_shape_gives_identical_results(require_gpu, shape, name, mo
     case = json.loads(str(z["params"]))
     out, info, _ = run_gpu(case, O.fields_from_golden(z))
     fused_ok = len(case.get("pulses", [])) == 0
-    assert info.launch_shape == (shape if (shape < 4 or fused_ok) else -1) or (shape == 4 and not fused_ok)
+    if shape < 4 or fused_ok:
+        assert info.launch_shape == shape
     for k in ("psi_plus", "n_plus"):
         if "out_" + k not in z.files or k not in out:
             continue
@@ -166,7 +167,7 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
     n = 1024
     wl = B.workload(n)
     res = {}
-    for shape in (2, 4):
+    for shape in (2, 4, 5, 6, 7, 8):
         monkeypatch.setenv("PHX_STAGE_SHAPE", str(shape))
         sp = B.system(pb, n, "f32", 0)
         sp.fft_every = 1e12
@@ -178,8 +179,9 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
             info = s.run(25)
             assert info.launch_shape == shape
             res[shape] = (s.get_field("psi_plus"), s.get_field("n_plus"))
-    np.testing.assert_array_equal(res[2][0], res[4][0])
-    np.testing.assert_array_equal(res[2][1], res[4][1])
+    for shape in (4, 5, 6, 7, 8):
+        np.testing.assert_array_equal(res[2][0], res[shape][0])
+        np.testing.assert_array_equal(res[2][1], res[shape][1])
 
 
 def test_bad_field_shape_is_rejected(require_gpu):
