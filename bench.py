@@ -144,11 +144,16 @@ def write_txt(path, arr, digits=9):
             np.savetxt(f, np.imag(arr), fmt=f"%.{digits}g")
 
 
-def reference_cpu_run(n, dtype, iters, wl):
-    """Run the reference CPU build (all host cores) for `iters` RK4 iterations of
-    the workload; returns (us_per_iteration, cores, binary) or None."""
+def reference_cpu_run(n, dtype, iters, wl, gpu=False):
+    """Run the reference build for `iters` RK4 iterations of the workload and
+    return (us_per_iteration, cores, binary) or None.  CPU build: all host
+    cores.  GPU build (gpu=True): the reference's own CUDA code for sm_100 on
+    this GPU, one subgrid (the like-for-like bar for the kernels)."""
     variant = "fp32" if dtype == "f32" else "fp64"
-    cand = [os.path.join(REF_BIN, f"phoenix_cpu_{variant}_v3"), os.path.join(REF_BIN, f"phoenix_cpu_{variant}")]
+    if gpu:
+        cand = [os.path.join(REF_BIN, f"phoenix_gpu_{variant}")]
+    else:
+        cand = [os.path.join(REF_BIN, f"phoenix_cpu_{variant}_v3"), os.path.join(REF_BIN, f"phoenix_cpu_{variant}")]
     binary = next((b for b in cand if os.path.exists(b)), None)
     if binary is None:
         return None
@@ -168,6 +173,8 @@ def reference_cpu_run(n, dtype, iters, wl):
                 repr(MASK_EVERY * dt * (1 - 1e-6)), "--initState", "load", files["psi0"], "1", "add", "both",
                 "--pump", "load", files["pump"], "1", "add", "both", "--potential", "load", files["potential"], "1",
                 "add", "both", "--fftMask", "load", files["mask"], "1", "add", "both"]
+        if gpu:
+            args += ["--subgrids", "1", "1"]
         proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
         m = re.search(r"-->\s*([0-9.eE+-]+)\s*mus/it", proc.stdout)
         if proc.returncode != 0 or not m:
@@ -230,7 +237,8 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--ref-iters", type=int, default=400, help="cap on reference CPU iterations")
     ap.add_argument("--cpu-iters", type=int, default=60, help="CPU-baseline sample in the phx arm")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu-iters", type=int, default=500, help="iterations of the reference GPU build")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU and GPU builds")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -400,6 +408,15 @@ def main():
                "sample": f"{args.cpu_iters if kind == 'reference' else 3} RK4 iterations of the {n}^2 workload "
                          f"with {what}"}
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        torch.cuda.synchronize()
+        res = reference_cpu_run(n, args.dtype, args.ref_gpu_iters, wl, gpu=True)
+        if res is not None:
+            ref_gpu = {"value": res[0], "unit": "us/iter", "binary": res[2], "iterations": args.ref_gpu_iters,
+                       "note": "the reference's own CUDA build for sm_100 on this GPU, --subgrids 1 1, wall clock "
+                               "of its main loop (its mus/it line)"}
+
     if rank == 0:
         us = step_ms * 1e3
         line = {"metric": METRIC, "value": us, "unit": "us/iter", "n_gpus": world, "steps": args.steps,
@@ -415,7 +432,7 @@ def main():
                              "step_alg_bytes": step_bytes,
                              "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},
                 "kernel_avg_ms": kernels_ms, "launch_shape": shape, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
-                "clocks": clocks.summary(), "cpu_baseline": cpu}
+                "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu}
         print(json.dumps(line))
     if dist:
         dist.barrier()
