@@ -21,6 +21,10 @@ Legs of the JSON line:
              region: algorithmic bytes / average duration vs measured HBM peak
   cpu_baseline  the reference's CPU build (PHOENIX compiled from its sources,
              oracle/_ref) on a bounded sample of the same workload, all host cores
+  sweep      the batched sweep: 256 independent 128^2..1024^2 FP32 instances
+             (pump 0.8-3.0x threshold, own disorder each) advanced by one
+             batch launch per iteration, against the same instances run one
+             after another through single-simulation handles
 `--impl reference` runs that reference CPU build alone (rank 0 of any launch).
 """
 from __future__ import annotations
@@ -219,6 +223,105 @@ def run_reference_arm(args):
     return 0
 
 
+SWEEP_SIZES = (128, 256, 512, 1024)
+
+
+def sweep_instances(count, seed=4):
+    """Config of the batched sweep: `count` independent instances, grid sizes
+    uniform over {128, 256, 512, 1024}^2, pump uniform in 0.8-3.0x threshold,
+    own disorder realisation of 0.05-0.2 meV rms (1 um correlation) each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.choice(SWEEP_SIZES))
+        p = float(rng.uniform(0.8, 3.0)) * P_TH
+        rms = float(rng.uniform(0.05, 0.2))
+        r = np.random.default_rng([seed, k])
+        x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n)
+        X, Y = np.meshgrid(x, x)
+        kk = 2 * np.pi * np.fft.fftfreq(n, d=L_BOX / (n - 1))
+        KX, KY = np.meshgrid(kk, kk)
+        pot = np.real(np.fft.ifft2(np.fft.fft2(r.standard_normal((n, n))) * np.exp(-(KX ** 2 + KY ** 2) / 2)))
+        pot *= rms / np.sqrt(np.mean(pot ** 2))
+        psi0 = 1e-2 * (r.standard_normal((n, n)) + 1j * r.standard_normal((n, n)))
+        out.append(dict(n=n, pump_factor=p / P_TH, rms=rms, psi0=psi0.astype(np.complex64),
+                        pump=(p * np.exp(-(X ** 2 + Y ** 2) / (2 * 10.0 ** 2))).astype(np.float32),
+                        potential=pot.astype(np.float32)))
+    return out
+
+
+def sweep_system(pb, n, device):
+    return pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                               periodic_boundary_y=True, dtype="f32", iterator="RK4", dt=dt_for(n), t0=0.0,
+                               t_max=1e12, pump_temporal=[pb.Temporal()], potential_temporal=[pb.Temporal()],
+                               device=device)
+
+
+def run_sweep(pb, torch, count, steps, device):
+    """Batched sweep vs the same instances run one after another through
+    single-simulation handles.  Both advance WARM + steps iterations from the
+    same inputs (WARM covers either path's launch-shape autotuning); the
+    timed part is `steps` iterations, CUDA events on the solvers' streams.
+    Every instance's final psi and n are compared bit for bit."""
+    warm = 22  # batch: 6 tuning + one 16-iteration graph; single: 18 tuning + 4
+    inst = sweep_instances(count)
+    zeros = {n: np.zeros((n, n), np.float32) for n in SWEEP_SIZES}
+    b = pb.BatchSolver([sweep_system(pb, d["n"], device) for d in inst])
+    for i, d in enumerate(inst):
+        b.set_field(i, "psi_plus", d["psi0"])
+        b.set_field(i, "n_plus", zeros[d["n"]])
+        b.set_field(i, "pump_plus", d["pump"])
+        b.set_field(i, "potential_plus", d["potential"])
+    bs = torch.cuda.ExternalStream(b.stream, device=device)
+    b.run(warm)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(bs):
+        e0.record(bs)
+    info = b.run(steps)
+    with torch.cuda.stream(bs):
+        e1.record(bs)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    got = [(b.get_field(i, "psi_plus"), b.get_field(i, "n_plus")) for i in range(count)]
+    shape = info.launch_shape
+    b.close()
+    seq_ms = 0.0
+    seq_wall = time.perf_counter()
+    equal = 0
+    for i, d in enumerate(inst):
+        s = pb.Solver(sweep_system(pb, d["n"], device))
+        s.set_field("psi_plus", d["psi0"])
+        s.set_field("n_plus", zeros[d["n"]])
+        s.set_field("pump_plus", d["pump"], 0)
+        s.set_field("potential_plus", d["potential"], 0)
+        s.run(warm)
+        st = torch.cuda.ExternalStream(s.stream, device=device)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            a0.record(st)
+        s.run(steps)
+        with torch.cuda.stream(st):
+            a1.record(st)
+        torch.cuda.synchronize()
+        seq_ms += a0.elapsed_time(a1)
+        equal += int(np.array_equal(got[i][0], s.get_field("psi_plus")) and
+                     np.array_equal(got[i][1], s.get_field("n_plus")))
+        s.close()
+    seq_wall = time.perf_counter() - seq_wall
+    points = sum(d["n"] ** 2 for d in inst)
+    return {"instances": count, "grid_points": points, "steps_timed": steps, "dtype": "f32",
+            "sizes": {str(n): sum(1 for d in inst if d["n"] == n) for n in SWEEP_SIZES},
+            "batch_ms": batch_ms, "batch_us_per_iteration": batch_ms * 1e3 / steps,
+            "batch_grid_point_updates_per_s": points * steps / (batch_ms * 1e-3),
+            "batch_tile_shape": shape,
+            "sequential_ms": seq_ms, "sequential_us_per_iteration": seq_ms * 1e3 / steps,
+            "sequential_wall_s_incl_setup": seq_wall,
+            "speedup_vs_sequential": seq_ms / batch_ms,
+            "bit_identical_instances": equal,
+            "note": "one batch launch per iteration (captured graphs of 16) vs 256 single-simulation handles "
+                    "run one after another; both device-timed over the same iterations"}
+
+
 def config_dict(args):
     return {"workload": f"rk4_scalar_reservoir_pump_potential_mask_{args.n}x{args.n}_{args.dtype}",
             "grid": [args.n, args.n], "iterator": "RK4", "boundary": "periodic", "dt_ps": dt_for(args.n),
@@ -236,9 +339,11 @@ def main():
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--ref-iters", type=int, default=400, help="cap on reference CPU iterations")
-    ap.add_argument("--cpu-iters", type=int, default=60, help="CPU-baseline sample in the phx arm")
+    ap.add_argument("--cpu-iters", type=int, default=1500, help="CPU-baseline sample in the phx arm (about 10 s)")
     ap.add_argument("--ref-gpu-iters", type=int, default=500, help="iterations of the reference GPU build")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU and GPU builds")
+    ap.add_argument("--sweep-instances", type=int, default=256, help="instances of the batched sweep (0: skip)")
+    ap.add_argument("--sweep-steps", type=int, default=200, help="timed iterations of the batched sweep")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -417,6 +522,10 @@ def main():
                        "note": "the reference's own CUDA build for sm_100 on this GPU, --subgrids 1 1, wall clock "
                                "of its main loop (its mus/it line)"}
 
+    sweep = None
+    if rank == 0 and args.sweep_instances > 0:
+        sweep = run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, local)
+
     if rank == 0:
         us = step_ms * 1e3
         line = {"metric": METRIC, "value": us, "unit": "us/iter", "n_gpus": world, "steps": args.steps,
@@ -432,7 +541,7 @@ def main():
                              "step_alg_bytes": step_bytes,
                              "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},
                 "kernel_avg_ms": kernels_ms, "launch_shape": shape, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
-                "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu}
+                "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu, "sweep": sweep}
         print(json.dumps(line))
     if dist:
         dist.barrier()

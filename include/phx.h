@@ -198,6 +198,35 @@ PHX_API phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_m
 /* The handle's cudaStream_t, as void*. */
 PHX_API phx_status phx_get_stream(phx_handle* h, void** stream);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent RK4 simulations -- pump-power sweeps, disorder
+ * realisations -- with their own grid sizes and parameters, advanced
+ * together.  The reference runs one simulation per process; the batch
+ * replaces n sequential runs of its main loop (source/main.cu:80-117).
+ * Every instance: scalar RK4, at most one pump and one potential group,
+ * constant temporal envelopes, no pulse, no k-space filter, one shared
+ * dtype.  One batch iteration advances every instance by one RK4 iteration
+ * in a single launch of a persistent kernel that walks the tiles of all
+ * instances; phx_batch_step replays a captured CUDA graph of it. */
+typedef struct phx_batch phx_batch;
+
+PHX_API phx_status phx_batch_create(const phx_params* instances, int32_t n_instances, phx_batch** out);
+PHX_API phx_status phx_batch_destroy(phx_batch* b);
+/* as phx_set_field / phx_get_field for one instance */
+PHX_API phx_status phx_batch_set_field(phx_batch* b, int32_t instance, int32_t field, int32_t group, const void* host,
+                                       int64_t count, int32_t host_dtype);
+PHX_API phx_status phx_batch_get_field(phx_batch* b, int32_t instance, int32_t field, int32_t group, void* host,
+                                       int64_t count, int32_t host_dtype);
+/* `iterations` batch iterations (every instance advances by that many RK4
+ * iterations; t_max is not consulted).  info->t / dt are instance 0's. */
+PHX_API phx_status phx_batch_step(phx_batch* b, int64_t iterations, phx_step_info* info);
+/* t and dt of one instance */
+PHX_API phx_status phx_batch_get_time(phx_batch* b, int32_t instance, double* t, double* dt);
+/* the batch's cudaStream_t, as void* */
+PHX_API phx_status phx_batch_get_stream(phx_batch* b, void** stream);
+/* message of the last failed call on this batch */
+PHX_API const char* phx_batch_last_error(const phx_batch* b);
+
 /* Message of the last failed call on this handle (or, when h is NULL, of
  * the last failed call in this thread that takes no handle: phx_create,
  * phx_sum_abs2_noalloc). */

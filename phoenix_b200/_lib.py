@@ -77,6 +77,14 @@ _SIGS = {
     "phx_last_error": (C.c_char_p, [C.c_void_p]),
     "phx_sum_abs2_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
                                        C.c_void_p, C.c_void_p]),
+    "phx_batch_create": (C.c_int, [C.POINTER(Params), C.c_int32, C.POINTER(C.c_void_p)]),
+    "phx_batch_destroy": (C.c_int, [C.c_void_p]),
+    "phx_batch_set_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),
+    "phx_batch_get_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),
+    "phx_batch_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(StepInfo)]),
+    "phx_batch_get_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "phx_batch_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "phx_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "phx_status_string": (C.c_char_p, [C.c_int32]),
     "phx_abi_version": (C.c_int32, []),
     "phx_build_info": (C.c_char_p, []),
@@ -110,4 +118,10 @@ def load():
 def check(status, handle=None):
     if status != PHX_OK:
         msg = load().phx_last_error(handle)
+        raise PhxError(status, msg.decode() if msg else "")
+
+
+def check_batch(status, batch=None):
+    if status != PHX_OK:
+        msg = load().phx_batch_last_error(batch)
         raise PhxError(status, msg.decode() if msg else "")

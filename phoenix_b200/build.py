@@ -35,20 +35,35 @@ def up_to_date():
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [NVCC] + ARCH_FLAGS + CFLAGS + ["-shared", "-o", LIB + ".tmp", os.path.join(CSRC, "phx_runtime.cu"),
-                                          os.path.join(CSRC, "phx_noalloc.cu"), "-lcufft"]
-    if ptxas_info:
-        cmd.insert(1, "-Xptxas=-v")
+UNITS = ["phx_runtime.cu", "phx_noalloc.cu", "phx_batch.cu"]
+OBJ_DIR = os.path.join(PKG, "_build")
+
+
+def _run(cmd, verbose):
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + proc.stdout[-8000:] + proc.stderr[-8000:])
+    return proc
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compile every translation unit (in parallel) and link libphx.so."""
+    if not force and up_to_date():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    extra = ["-Xptxas=-v"] if ptxas_info else []
+    objs = [os.path.join(OBJ_DIR, u.replace(".cu", ".o")) for u in UNITS]
+    cmds = [[NVCC] + extra + ARCH_FLAGS + CFLAGS + ["-c", "-o", o, os.path.join(CSRC, u)] for u, o in zip(UNITS, objs)]
+    with ThreadPoolExecutor(len(cmds)) as ex:
+        procs = list(ex.map(lambda c: _run(c, verbose), cmds))
     if ptxas_info or verbose:
-        sys.stderr.write(proc.stderr)
+        for p in procs:
+            sys.stderr.write(p.stderr)
+    _run([NVCC] + ARCH_FLAGS + ["-shared", "-o", LIB + ".tmp"] + objs + ["-lcufft"], verbose)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

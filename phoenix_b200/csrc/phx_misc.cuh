@@ -214,7 +214,7 @@ __global__ void ring7_kernel(const cx<T>* __restrict__ psi0, long long pitch, in
 }
 
 // Sum of n (error, norm) pairs in a fixed order: one block, deterministic.
-__global__ void finalize_pairs_kernel(const double* __restrict__ partials, long long n, double* __restrict__ out) {
+static __global__ void finalize_pairs_kernel(const double* __restrict__ partials, long long n, double* __restrict__ out) {
     __shared__ double sa[32], sb[32];
     double a = 0.0, b = 0.0;
     for (long long i = threadIdx.x; i < n; i += blockDim.x) {

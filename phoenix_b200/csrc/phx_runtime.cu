@@ -29,66 +29,11 @@
 #include "phx_stage_tetm.cuh"
 #include "phx_step_fused.cuh"
 #include "phx_step_tma.cuh"
+#include "phx_rt.hpp"
 
 namespace phx {
 
 thread_local std::string g_create_error;
-
-struct Error {
-    phx_status status;
-    std::string msg;
-};
-
-#define PHX_CUDA(call)                                                                                       \
-    do {                                                                                                     \
-        cudaError_t e_ = (call);                                                                             \
-        if (e_ != cudaSuccess) throw Error{PHX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
-    } while (0)
-#define PHX_CUFFT(call)                                                                       \
-    do {                                                                                      \
-        cufftResult r_ = (call);                                                              \
-        if (r_ != CUFFT_SUCCESS) throw Error{PHX_ERR_CUDA, std::string(#call) + " failed (" + \
-                                             std::to_string((int)r_) + ")"};                  \
-    } while (0)
-
-static void fail(phx_status s, const std::string& m) { throw Error{s, m}; }
-
-// ---------------------------------------------------------------- device memory
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    void alloc(size_t n, cudaStream_t s) {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = n;
-        if (n == 0) return;
-        cudaError_t e = cudaMalloc(&p, n);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            (void)cudaGetLastError();
-            fail(PHX_ERR_OOM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
-        }
-        PHX_CUDA(cudaMemsetAsync(p, 0, n, s));
-    }
-};
-
-struct PinnedBuf {
-    void* p = nullptr;
-    ~PinnedBuf() {
-        if (p) cudaFreeHost(p);
-    }
-    void alloc(size_t n) {
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        PHX_CUDA(cudaMallocHost(&p, n));
-    }
-};
 
 // ---------------------------------------------------------------- engine
 struct EngineBase {
@@ -600,29 +545,9 @@ struct Engine final : EngineBase {
         rk4_fused_kernel<T, RES, TW, TH, NT><<<grid, NT, 0, stream>>>(F);
     }
     // ---- TMA-fed persistent variant
-    using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-    EncodeFn encode = nullptr;
     int tma_blocks_per_sm = 0, sm_count = 0;
     void tensor_map(CUtensorMap* m, void* alloc_base, bool complex, int box_w_points, int box_h) {
-        if (!encode) {
-            cudaDriverEntryPointQueryResult q;
-            void* fn = nullptr;
-            PHX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-            if (q != cudaDriverEntryPointSuccess || !fn) fail(PHX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
-            encode = reinterpret_cast<EncodeFn>(fn);
-        }
-        const int per = complex ? 2 : 1;
-        const cuuint64_t dims[2] = {(cuuint64_t)(per * pitch), (cuuint64_t)rows};
-        const cuuint64_t strides[1] = {(cuuint64_t)(per * pitch * sizeof(T))};
-        const cuuint32_t box[2] = {(cuuint32_t)(per * box_w_points), (cuuint32_t)box_h};
-        const cuuint32_t estr[2] = {1, 1};
-        const CUresult r = encode(m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2,
-                                  alloc_base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) fail(PHX_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+        plane_tensor_map<T>(m, alloc_base, complex, pitch, rows, box_w_points, box_h);
     }
     template <bool RES, int TW, int TH, int NT>
     void go_tma(const FusedParams<T>& F) {
@@ -683,8 +608,6 @@ struct Engine final : EngineBase {
     }
     bool step_rk4_fused() {
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
-        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
-        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
         FusedParams<T> F;
         std::memset(&F, 0, sizeof(F));
         for (int s = 0; s < 4; ++s) {
@@ -698,32 +621,18 @@ struct Engine final : EngineBase {
                 if (c.imag() != (T)0) return false;
                 F.pot_c[s] = c.real();
             }
-            F.b[s] = bw[s];
-            if (s < 3) F.dtw[s] = dt * aw[s];
         }
         if (!psi_alt.p) {
             psi_alt.alloc(sizeof(C) * plane, stream);
             n_alt.alloc(sizeof(T) * plane, stream);
         }
-        F.N_r = N_r;
-        F.N_c = N_c;
-        F.img_x = P.periodic_x;
-        F.img_y = P.periodic_y;
-        F.pitch = pitch;
+        fused_constants<T>(F, P, d, dt, pitch);
         F.psi0 = cplane(psi[0]);
         F.n0 = rplane(nres[0]);
         F.psi1 = cplane(psi_alt);
         F.n1 = rplane(n_alt);
         F.pump = P.n_pump_groups ? rplane(pump[0]) : nullptr;
         F.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
-        F.m2 = d.m2, F.odx2 = d.odx2, F.ody2 = d.ody2, F.meff = d.meff, F.ohb = d.ohb;
-        F.ohb_gc = d.ohb * (T)P.g_c;
-        F.half_gamma_c = (T)0.5 * (T)P.gamma_c;
-        F.ohb_gr = d.ohb * (T)P.g_r;
-        F.half_R = (T)0.5 * (T)P.R;
-        F.gamma_r = (T)P.gamma_r;
-        F.R = (T)P.R;
-        F.dt = dt;
         cudaEvent_t a = nullptr;
         prof_begin(a);
         if (P.use_reservoir)

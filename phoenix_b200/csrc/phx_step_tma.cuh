@@ -89,13 +89,64 @@ struct TmaLayout {
     static constexpr int pump_off = n_off + al(real_bytes);
     static constexpr int pot_off = pump_off + al(real_bytes);
     static constexpr int slot_bytes = pot_off + al(real_bytes);
-    static constexpr int b_off = 2 * slot_bytes;            // stage ping-pong buffer B
-    static constexpr int bar_off = b_off + al(psi_bytes);   // two mbarriers
-    static constexpr int total = bar_off + 16 + 128;  // + slack to align the base to 128 bytes
+    // stage buffers B and C: rows of SW points with one leading pad point, so
+    // that the point pairs a thread owns start on 16-byte boundaries
+    static constexpr int SW = W4 + 2;
+    static constexpr int pad_bytes = SW * H4 * 2 * (int)sizeof(T);
+    static constexpr int b_off = 2 * slot_bytes;
+    static constexpr int c_off = b_off + al(pad_bytes);
+    static constexpr int bar_off = c_off + al(pad_bytes);  // two mbarriers
+    static constexpr int total = bar_off + 16 + 128;       // + slack to align the base to 128 bytes
 };
 
-template <typename T, bool RES, int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ TmaParams<T> Q) {
+// Order earlier generic-proxy writes of a tensor map in global memory before
+// its use by the tensor-map proxy (maps written by a host copy before the
+// launch need nothing more).
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
+}
+
+// 16-byte shared-memory access to the point pair at an even index
+template <typename T>
+__device__ __forceinline__ void lds_pair(const cx<T>* p, cx<T>& a, cx<T>& b) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        a = mk(v.x, v.y);
+        b = mk(v.z, v.w);
+    } else {
+        a = p[0];
+        b = p[1];
+    }
+}
+template <typename T>
+__device__ __forceinline__ void sts_pair(cx<T>* p, cx<T> a, cx<T> b) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(a.re, a.im, b.re, b.im);
+    } else {
+        p[0] = a;
+        p[1] = b;
+    }
+}
+
+// What one tile needs: its tensor maps, its parameters and its origin.
+template <typename T>
+struct TileRef {
+    const CUtensorMap* psi_map;
+    const CUtensorMap* n_map;
+    const CUtensorMap* pump_map;
+    const CUtensorMap* pot_map;
+    const FusedParams<T>* f;
+    int has_pump, has_pot;
+    int tx0, ty0;
+};
+
+// Persistent tile loop shared by the single-simulation and the batched
+// kernel; `tile_of(g)` returns the TileRef of global tile g.  BATCH: the
+// tensor maps and parameters live in global memory (one set per instance);
+// the maps are acquired for the tensor-map proxy before use and the tile's
+// parameters are staged in shared memory.
+template <typename T, bool RES, int TW, int TH, int NT, bool BATCH, typename TileOf>
+__device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles, int* err) {
     using Lay = TmaLayout<T, TW, TH>;
     constexpr int W4 = Lay::W4, WR = Lay::WR;
     constexpr int W3 = TW + 6, H3 = TH + 6;
@@ -107,22 +158,29 @@ __global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ Tma
     unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + Lay::bar_off);
     cx<T>* sB = reinterpret_cast<cx<T>*>(smem + Lay::b_off);
-    const FusedParams<T>& P = Q.f;
-    const bool has_pump = Q.has_pump != 0, has_pot = Q.has_pot != 0;
-    const long long pitch = P.pitch;
-    const unsigned tx_bytes = (unsigned)Lay::psi_bytes + (unsigned)Lay::real_bytes * (RES ? 1u : 0u) +
-                              (unsigned)Lay::real_bytes * ((RES && has_pump) ? 1u : 0u) +
-                              (unsigned)Lay::real_bytes * (has_pot ? 1u : 0u);
+    cx<T>* sC = reinterpret_cast<cx<T>*>(smem + Lay::c_off);
+    constexpr int SW = Lay::SW;
 
-    auto issue = [&](int slot, int tile) {
+    __shared__ FusedParams<T> sP;  // BATCH: this tile's parameters
+
+    auto issue = [&](int slot, int g) {
+        const TileRef<T> R = tile_of(g);
+        if constexpr (BATCH) {
+            tensormap_acquire(R.psi_map);
+            if (RES) tensormap_acquire(R.n_map);
+            if (RES && R.has_pump) tensormap_acquire(R.pump_map);
+            if (R.has_pot) tensormap_acquire(R.pot_map);
+        }
         unsigned char* base = smem + slot * Lay::slot_bytes;
-        const int ty0 = (tile / Q.tiles_x) * TH, tx0 = (tile % Q.tiles_x) * TW;
+        const unsigned tx_bytes = (unsigned)Lay::psi_bytes + (unsigned)Lay::real_bytes * (RES ? 1u : 0u) +
+                                  (unsigned)Lay::real_bytes * ((RES && R.has_pump) ? 1u : 0u) +
+                                  (unsigned)Lay::real_bytes * (R.has_pot ? 1u : 0u);
         mbar_expect_tx(&bars[slot], tx_bytes);
         // psi: x in T units (2 per point) of the padded plane, ring kRing
-        tma_load_2d(base + Lay::psi_off, &Q.psi_map, 2 * (tx0 - 4 + kRing), ty0 - 4 + kRing, &bars[slot]);
-        if (RES) tma_load_2d(base + Lay::n_off, &Q.n_map, tx0 - 4 + kRing, ty0 - 3 + kRing, &bars[slot]);
-        if (RES && has_pump) tma_load_2d(base + Lay::pump_off, &Q.pump_map, tx0 - 4 + kRing, ty0 - 3 + kRing, &bars[slot]);
-        if (has_pot) tma_load_2d(base + Lay::pot_off, &Q.pot_map, tx0 - 4 + kRing, ty0 - 3 + kRing, &bars[slot]);
+        tma_load_2d(base + Lay::psi_off, R.psi_map, 2 * (R.tx0 - 4 + kRing), R.ty0 - 4 + kRing, &bars[slot]);
+        if (RES) tma_load_2d(base + Lay::n_off, R.n_map, R.tx0 - 4 + kRing, R.ty0 - 3 + kRing, &bars[slot]);
+        if (RES && R.has_pump) tma_load_2d(base + Lay::pump_off, R.pump_map, R.tx0 - 4 + kRing, R.ty0 - 3 + kRing, &bars[slot]);
+        if (R.has_pot) tma_load_2d(base + Lay::pot_off, R.pot_map, R.tx0 - 4 + kRing, R.ty0 - 3 + kRing, &bars[slot]);
     };
 
     if (threadIdx.x == 0) {
@@ -133,33 +191,45 @@ __global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ Tma
     }
     __syncthreads();
     int tile = blockIdx.x;
-    if (threadIdx.x == 0 && tile < Q.n_tiles) issue(0, tile);
+    if (threadIdx.x == 0 && tile < n_tiles) issue(0, tile);
     int it = 0;
     bool pending_next = false;  // thread 0: a load into the other slot is in flight
-    for (; tile < Q.n_tiles; tile += gridDim.x, ++it) {
+    for (; tile < n_tiles; tile += gridDim.x, ++it) {
         const int slot = it & 1;
         const unsigned parity = (unsigned)((it >> 1) & 1);
         const int next = tile + gridDim.x;
         if (threadIdx.x == 0) {
-            pending_next = next < Q.n_tiles;
+            pending_next = next < n_tiles;
             if (pending_next) issue(slot ^ 1, next);
+        }
+        const TileRef<T> R = tile_of(tile);
+        if constexpr (BATCH) {
+            // the previous tile's reads of sP ended at its closing barrier
+            constexpr int kWords = (int)(sizeof(FusedParams<T>) / sizeof(int));
+            static_assert(sizeof(FusedParams<T>) % sizeof(int) == 0, "FusedParams copied as words");
+            const int* src = reinterpret_cast<const int*>(R.f);
+            int* dst = reinterpret_cast<int*>(&sP);
+            for (int w = threadIdx.x; w < kWords; w += NT) dst[w] = __ldg(src + w);
         }
         const bool ok = mbar_wait_bounded(&bars[slot], parity);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
-                atomicExch(Q.err, 1);
+                atomicExch(err, 1);
                 // drain this CTA's loads still in flight before leaving
                 (void)mbar_wait_bounded(&bars[slot], parity);
                 if (pending_next) (void)mbar_wait_bounded(&bars[slot ^ 1], (unsigned)(((it + 1) >> 1) & 1));
             }
             return;
         }
+        const FusedParams<T>& P = BATCH ? sP : *R.f;
+        const bool has_pump = R.has_pump != 0, has_pot = R.has_pot != 0;
+        const long long pitch = P.pitch;
         unsigned char* base = smem + slot * Lay::slot_bytes;
         cx<T>* sA = reinterpret_cast<cx<T>*>(base + Lay::psi_off);
         const T* s_n = reinterpret_cast<const T*>(base + Lay::n_off);
         const T* s_pu = reinterpret_cast<const T*>(base + Lay::pump_off);
         const T* s_po = reinterpret_cast<const T*>(base + Lay::pot_off);
-        const int ty0 = (tile / Q.tiles_x) * TH, tx0 = (tile % Q.tiles_x) * TW;
+        const int ty0 = R.ty0, tx0 = R.tx0;
 
         cx<T> y0[OWN][2], acc[OWN][2];
         T n0[OWN][2], ns[OWN][2], an[OWN][2];
@@ -175,34 +245,40 @@ __global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ Tma
                 ns[j][h] = n0[j][h];
             }
         }
+        // stage 0 reads the TMA box sA (row W4, unpadded); stages 1-3 ping-pong
+        // between the padded buffers: 0: sA -> sB, 1: sB -> sC, 2: sC -> sB, 3: sB -> global
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
-            const cx<T>* in = (s & 1) ? sB : sA;
-            cx<T>* out = (s & 1) ? sA : sB;
+            const cx<T>* in = s == 0 ? sA : (s == 2 ? sC : sB);
+            cx<T>* out = s == 1 ? sC : sB;
 #pragma unroll
             for (int j = 0; j < OWN; ++j) {
                 const int p = threadIdx.x + NT * j;
                 const int qy = p / PW, qx = 2 * (p - qy * PW);
                 if (p >= NP || qy < s || qy >= H3 - s || qx + 1 < s || qx >= W3 - s) continue;
-                const int e = (qy + 1) * W4 + qx + 1;
+                const int ep = (qy + 1) * SW + qx + 2;  // padded index of the pair (even)
                 const int er = qy * WR + qx + 1;
-                cx<T> c0, c1;
+                cx<T> c0, c1, u0, u1, d0, d1, lft, rgt;
                 if (s == 0) {
+                    const int e = (qy + 1) * W4 + qx + 1;
                     c0 = y0[j][0];
                     c1 = y0[j][1];
+                    u0 = in[e - W4], u1 = in[e - W4 + 1];
+                    d0 = in[e + W4], d1 = in[e + W4 + 1];
+                    lft = in[e - 1], rgt = in[e + 2];
                 } else {
-                    c0 = in[e];
-                    c1 = in[e + 1];
+                    lds_pair(in + ep, c0, c1);
+                    lds_pair(in + ep - SW, u0, u1);
+                    lds_pair(in + ep + SW, d0, d1);
+                    lft = in[ep - 1], rgt = in[ep + 2];
                 }
-                const cx<T> u0 = in[e - W4], u1 = in[e - W4 + 1];
-                const cx<T> d0 = in[e + W4], d1 = in[e + W4 + 1];
-                const cx<T> lft = in[e - 1], rgt = in[e + 2];
                 const T pu0 = (RES && has_pump) ? s_pu[er] : (T)0, pu1 = (RES && has_pump) ? s_pu[er + 1] : (T)0;
                 const T po0 = has_pot ? s_po[er] : (T)0, po1 = has_pot ? s_po[er + 1] : (T)0;
                 cx<T> kw[2];
                 T kr[2] = {(T)0, (T)0};
                 rhs_fused<T, RES>(P, s, c0, u0, d0, lft, c1, ns[j][0], pu0, po0, has_pump, has_pot, kw[0], kr[0]);
                 rhs_fused<T, RES>(P, s, c1, u1, d1, c0, rgt, ns[j][1], pu1, po1, has_pump, has_pot, kw[1], kr[1]);
+                cx<T> o[2];
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     if (s == 0) {
@@ -213,7 +289,7 @@ __global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ Tma
                         an[j][h] = radd(an[j][h], rmul(P.b[s], kr[h]));
                     }
                     if (s < 3) {
-                        out[e + h] = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
+                        o[h] = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
                         if constexpr (RES) ns[j][h] = radd(n0[j][h], rmul(P.dtw[s], kr[h]));
                     } else {
                         const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
@@ -230,6 +306,7 @@ __global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ Tma
                         }
                     }
                 }
+                if (s < 3) sts_pair(out + ep, o[0], o[1]);
             }
             __syncthreads();
         }
@@ -238,6 +315,65 @@ __global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ Tma
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
     }
+}
+
+template <typename T, bool RES, int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ TmaParams<T> Q) {
+    auto tile_of = [&](int g) {
+        TileRef<T> R;
+        R.psi_map = &Q.psi_map;
+        R.n_map = &Q.n_map;
+        R.pump_map = &Q.pump_map;
+        R.pot_map = &Q.pot_map;
+        R.f = &Q.f;
+        R.has_pump = Q.has_pump;
+        R.has_pot = Q.has_pot;
+        R.ty0 = (g / Q.tiles_x) * TH;
+        R.tx0 = (g % Q.tiles_x) * TW;
+        return R;
+    };
+    tma_tile_loop<T, RES, TW, TH, NT, false>(tile_of, Q.n_tiles, Q.err);
+}
+
+// ---------------------------------------------------------------- batches
+// Every instance of a batch owns two state planes (A, B); iteration k reads
+// A and writes B when k is even, the other way round when odd.  Its tensor
+// maps and parameters for both directions live in device memory.
+template <typename T>
+struct alignas(64) BatchInstance {
+    CUtensorMap maps[2][4];  // [direction][psi, n, pump, potential]
+    FusedParams<T> f[2];     // [direction]
+    int has_pump, has_pot;
+    int tiles_x, tile_begin;
+};
+
+template <typename T>
+struct BatchParams {
+    const BatchInstance<T>* inst;
+    const int* tile_inst;  // global tile -> instance
+    int n_tiles;
+    int dir;
+    int* err;
+};
+
+template <typename T, bool RES, int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) rk4_batch_kernel(const __grid_constant__ BatchParams<T> B) {
+    auto tile_of = [&](int g) {
+        const BatchInstance<T>& I = B.inst[__ldg(B.tile_inst + g)];
+        TileRef<T> R;
+        R.psi_map = &I.maps[B.dir][0];
+        R.n_map = &I.maps[B.dir][1];
+        R.pump_map = &I.maps[B.dir][2];
+        R.pot_map = &I.maps[B.dir][3];
+        R.f = &I.f[B.dir];
+        R.has_pump = I.has_pump;
+        R.has_pot = I.has_pot;
+        const int local = g - I.tile_begin;
+        R.ty0 = (local / I.tiles_x) * TH;
+        R.tx0 = (local % I.tiles_x) * TW;
+        return R;
+    };
+    tma_tile_loop<T, RES, TW, TH, NT, true>(tile_of, B.n_tiles, B.err);
 }
 
 }  // namespace phx

@@ -56,3 +56,33 @@ def test_null_handle_calls_fail_cleanly():
 def test_unknown_iterator_is_rejected_like_the_factory():
     with pytest.raises(KeyError):
         pb.SystemParameters(iterator="RK17").to_abi()
+
+
+def _batch_status(systems):
+    lib = L.load()
+    b = C.c_void_p()
+    arr = (L.Params * len(systems))(*[s.to_abi() for s in systems])
+    st = lib.phx_batch_create(arr, len(systems), C.byref(b))
+    assert not b.value
+    return st, lib.phx_batch_last_error(None).decode()
+
+
+def test_batch_rejects_unsupported_instances_without_device_work():
+    ok = pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f32", use_reservoir=True)
+    cases = [
+        (pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f64", use_reservoir=True), 1, "dtype"),
+        (pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f32", use_reservoir=False), 1, "use_reservoir"),
+        (pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f32", use_reservoir=True, iterator="DP45"), 6, "RK4"),
+        (pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f32", use_reservoir=True, use_twin_mode=True), 6, "scalar"),
+        (pb.SystemParameters(N_c=63, N_r=64, dt=0.01, dtype="f32", use_reservoir=True), 6, "even"),
+        (pb.SystemParameters(N_c=4, N_r=64, dt=0.01, dtype="f32", use_reservoir=True), 1, "8 x 8"),
+    ]
+    for bad, status, words in cases:
+        st, msg = _batch_status([ok, bad])
+        assert st == status, (msg, status)
+        assert msg.startswith("instance 1") and words in msg, msg
+    lib = L.load()
+    b = C.c_void_p()
+    assert lib.phx_batch_create(None, 1, C.byref(b)) == 1
+    assert lib.phx_batch_step(None, 1, None) == 1
+    assert lib.phx_batch_destroy(None) == 0
