@@ -25,6 +25,8 @@ Legs of the JSON line:
              (pump 0.8-3.0x threshold, own disorder each) advanced by one
              batch launch per iteration, against the same instances run one
              after another through single-simulation handles
+  adjoint    the inverse-design gradient: 512^2 FP32, 500 RK4 iterations, device
+             time of the plain forward, the checkpointed forward and the backward
 `--impl reference` runs that reference CPU build alone (rank 0 of any launch).
 """
 from __future__ import annotations
@@ -322,6 +324,71 @@ def run_sweep(pb, torch, count, steps, device):
                     "run one after another; both device-timed over the same iterations"}
 
 
+def run_adjoint(pb, torch, device, iters=500, n=512):
+    """Inverse-design configuration: 512^2 FP32 RK4, T = 500, dt = 0.04 ps,
+    pump disc of 1.2x threshold (radius 30 um), loss sum (|psi_T|^2 - rho)^2 dV
+    against seven Gaussian spots on a hexagonal lattice.  Device time of the
+    plain forward (phx_step), of the checkpointed forward and of the backward
+    (recompute + vector-Jacobian kernels), CUDA events on the solver stream."""
+    from phoenix_b200.adjoint import evolve
+
+    sp = pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, g_pm=0.0, delta_LT=0.0,
+                             periodic_boundary_x=True, periodic_boundary_y=True, dtype="f32", iterator="RK4",
+                             dt=0.04, t_max=1e12, fft_every=1e12, pump_temporal=[pb.Temporal()], device=device)
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n)
+    X, Y = np.meshgrid(x, x)
+    pump = np.where(X ** 2 + Y ** 2 <= 30.0 ** 2, 1.2 * P_TH, 0.0).astype(np.float32)
+    rho = np.zeros((n, n))
+    for x0, y0 in [(0.0, 0.0)] + [(15 * np.cos(a), 15 * np.sin(a)) for a in np.arange(6) * np.pi / 3]:
+        rho += 5.0 * np.exp(-((X - x0) ** 2 + (Y - y0) ** 2) / (2 * 4.0 ** 2))
+    rng = np.random.default_rng(6)
+    psi0 = (1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
+    dev = f"cuda:{device}"
+    s = pb.Solver(sp)
+    st = torch.cuda.ExternalStream(s.stream, device=device)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    # plain forward (after autotuning)
+    s.set_field("psi_plus", psi0)
+    s.set_field("pump_plus", pump, 0)
+    s.run(40)
+    a, b = ev(), ev()
+    with torch.cuda.stream(st):
+        a.record(st)
+    s.run(iters)
+    with torch.cuda.stream(st):
+        b.record(st)
+    torch.cuda.synchronize()
+    plain_ms = a.elapsed_time(b)
+    P = torch.tensor(pump, device=dev, requires_grad=True)
+    z0 = torch.tensor(psi0, device=dev)
+    m0 = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    rho_t = torch.tensor(rho, dtype=torch.float32, device=dev)
+    dV = (L_BOX / (n - 1)) ** 2
+    times = []
+    for _ in range(2):  # the first pass allocates the segment planes
+        P.grad = None
+        e0, e1, e2 = ev(), ev(), ev()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(st):
+            e0.record(st)
+        psi_T, _ = evolve(s, P, z0, m0, iters)
+        with torch.cuda.stream(st):
+            e1.record(st)
+        L = (((psi_T.real ** 2 + psi_T.imag ** 2) - rho_t) ** 2).sum() * dV
+        L.backward()
+        with torch.cuda.stream(st):
+            e2.record(st)
+        torch.cuda.synchronize()
+        times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+    s.close()
+    fwd, bwd = times[-1]
+    return {"grid": [n, n], "iterations": iters, "dtype": "f32", "checkpoint_every": int(np.ceil(np.sqrt(iters))),
+            "plain_forward_ms": plain_ms, "checkpointed_forward_ms": fwd, "backward_ms": bwd,
+            "backward_over_plain_forward": bwd / plain_ms,
+            "note": "backward = recompute of every segment with the stage kernels + 4 vector-Jacobian launches per "
+                    "iteration; loss evaluation by torch between the two"}
+
+
 def config_dict(args):
     return {"workload": f"rk4_scalar_reservoir_pump_potential_mask_{args.n}x{args.n}_{args.dtype}",
             "grid": [args.n, args.n], "iterator": "RK4", "boundary": "periodic", "dt_ps": dt_for(args.n),
@@ -344,6 +411,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU and GPU builds")
     ap.add_argument("--sweep-instances", type=int, default=256, help="instances of the batched sweep (0: skip)")
     ap.add_argument("--sweep-steps", type=int, default=200, help="timed iterations of the batched sweep")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (inverse-design) leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -525,6 +593,9 @@ def main():
     sweep = None
     if rank == 0 and args.sweep_instances > 0:
         sweep = run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, local)
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        adjoint = run_adjoint(pb, torch, local)
 
     if rank == 0:
         us = step_ms * 1e3
@@ -541,7 +612,8 @@ def main():
                              "step_alg_bytes": step_bytes,
                              "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},
                 "kernel_avg_ms": kernels_ms, "launch_shape": shape, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
-                "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu, "sweep": sweep}
+                "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu, "sweep": sweep,
+                "adjoint": adjoint}
         print(json.dumps(line))
     if dist:
         dist.barrier()

@@ -198,6 +198,33 @@ PHX_API phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_m
 /* The handle's cudaStream_t, as void*. */
 PHX_API phx_status phx_get_stream(phx_handle* h, void** stream);
 
+/* ---------------------------------------------------------------- device memory
+ * No counterpart in the reference (its fields move through host matrices,
+ * cuda_matrix.cuh:445-476).  Copy one field between the handle and a
+ * caller-owned contiguous N_r x N_c device array in the build precision
+ * (complex fields as interleaved (re, im)); `count` is the number of real
+ * values.  Ordered on the handle's stream; an upload rebuilds the plane's
+ * ring (periodic images / zeros).  For torch tensors and other device-side
+ * callers. */
+PHX_API phx_status phx_set_field_device(phx_handle* h, int32_t field, int32_t group, const void* dev, int64_t count);
+PHX_API phx_status phx_get_field_device(phx_handle* h, int32_t field, int32_t group, void* dev, int64_t count);
+
+/* ---------------------------------------------------------------- adjoint
+ * No counterpart in the reference.  Reverse-mode gradients of scalar
+ * fixed-step RK4 (periodic boundaries, constant envelopes, at most one pump
+ * and one potential group, no pulse, no filter, no noise).
+ * phx_adjoint_forward runs `iterations` iterations from the handle's state
+ * (as phx_step does) and keeps a checkpoint of the state every
+ * `checkpoint_every` iterations (<= 0: ceil(sqrt(iterations))).
+ * phx_adjoint_backward takes dL/dpsi_T (and dL/dn_T, or NULL for zero) of
+ * the final state and writes dL/dpsi_0, dL/dn_0 and dL/dP (pump group 0) --
+ * each may be NULL -- by recomputing one checkpoint segment at a time.  All
+ * arrays are contiguous N_r x N_c device arrays in the build precision; the
+ * adjoint of a complex value u + iv is dL/du + i dL/dv. */
+PHX_API phx_status phx_adjoint_forward(phx_handle* h, int64_t iterations, int64_t checkpoint_every);
+PHX_API phx_status phx_adjoint_backward(phx_handle* h, const void* dpsi_T, const void* dn_T, void* dpsi_0, void* dn_0,
+                                        void* dpump);
+
 /* ---------------------------------------------------------------- batches
  * Many independent RK4 simulations -- pump-power sweeps, disorder
  * realisations -- with their own grid sizes and parameters, advanced

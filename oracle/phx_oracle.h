@@ -22,9 +22,12 @@
  * in the reference's storage layout (halo-padded arrays, complex reservoir,
  * k-stack), so halo-cell behaviour (zero boundaries, DP45 error norms over
  * padded cells, buffer swaps) is reproduced as the reference has it.
- * Stochastic noise is not restated (the reference draws it from cuRAND /
- * a shared mt19937 and is not reproducible); imaginary-time propagation is
- * not on the path.
+ * Stochastic noise (--dw) is restated with the reference's distribution and
+ * placement (gp_scalar stochastic terms, the dw term of the stage sums,
+ * kernel_summation.cuh:216-224, one complex normal field per iteration
+ * shared by both polarisations) but drawn from a counter-based generator
+ * (phx_oracle.c), since the reference's cuRAND / mt19937 stream is not
+ * reproducible.  Imaginary-time propagation is not on the path.
  */
 #ifndef PHX_ORACLE_H
 #define PHX_ORACLE_H
@@ -62,6 +65,8 @@ typedef struct {
     phx_oracle_temporal pump_t[PHX_ORACLE_MAX_GROUPS];
     phx_oracle_temporal potential_t[PHX_ORACLE_MAX_GROUPS];
     phx_oracle_temporal pulse_t[PHX_ORACLE_MAX_GROUPS];
+    double stochastic_amplitude; /* --dw; noise is on when > 0 */
+    uint64_t seed;
 } phx_oracle_params;
 
 /* Derived kernel constants as calculateAuto computes them (system.cpp:116-160),
@@ -76,6 +81,9 @@ typedef struct {
 } phx_oracle_result;
 
 void phx_oracle_derive_f64(const phx_oracle_params* p, phx_oracle_derived* d);
+/* the noise generator: Philox4x32-10 in place on ctr, and one normal pair */
+void phx_oracle_philox4x32_10(uint32_t ctr[4], uint32_t k0, uint32_t k1);
+void phx_oracle_noise_normal2(uint64_t seed, uint64_t iteration, uint32_t point, float* z0, float* z1);
 void phx_oracle_derive_f32(const phx_oracle_params* p, phx_oracle_derived* d);
 
 /* Fields are full N_r x N_c row-major grids (column index fastest).  Complex

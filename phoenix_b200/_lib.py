@@ -77,6 +77,10 @@ _SIGS = {
     "phx_last_error": (C.c_char_p, [C.c_void_p]),
     "phx_sum_abs2_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
                                        C.c_void_p, C.c_void_p]),
+    "phx_set_field_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
+    "phx_get_field_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
+    "phx_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64]),
+    "phx_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "phx_batch_create": (C.c_int, [C.POINTER(Params), C.c_int32, C.POINTER(C.c_void_p)]),
     "phx_batch_destroy": (C.c_int, [C.c_void_p]),
     "phx_batch_set_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),

@@ -26,6 +26,8 @@ __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float rsqrt_rn(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double rsqrt_rn(double a) { return __dsqrt_rn(a); }
 
 template <typename T>
 __device__ __forceinline__ cx<T> mk(T re, T im) {

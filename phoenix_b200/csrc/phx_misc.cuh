@@ -4,6 +4,7 @@
 #pragma once
 
 #include "phx_device.cuh"
+#include "phx_noise.cuh"
 
 namespace phx {
 
@@ -109,6 +110,10 @@ struct RingParams {
     T e[7];            // error weights
     int passes;        // 1, or 2 where the reference counts the plus error twice
     double* partials;  // per-block (error, norm)
+    // stochastic dw term of the stage sums (as in the stage kernels)
+    NoiseParams noise;
+    T noise_amp, w_sum[7], R, gamma_c, four_dV, noise_scale;
+    const T* n0;       // state reservoir, or nullptr without reservoir
 };
 
 template <typename T>
@@ -150,6 +155,11 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
             cx<T> acc = smul(R.a[m - 1][0], R.k[idx]);
             for (int q = 1; q < R.nw[m - 1]; ++q) acc = cadd(acc, smul(R.a[m - 1][q], R.k[(long long)q * R.plane + idx]));
             y = cadd(y0, smul(R.dt, acc));
+        }
+        if (R.noise.on) {
+            const cx<T> xi = noise_xi(R.noise, noise_point(r, c, R.N_r, R.N_c, R.periodic_x, R.periodic_y), R.noise_amp);
+            const T s_ = R.n0 ? rsqrt_rn(rdiv(radd(rmul(R.R, R.n0[idx]), R.gamma_c), R.four_dV)) : R.noise_scale;
+            y = cadd(y, mk(rmul(rmul(R.w_sum[m - 1], xi.re), s_), rmul(rmul(R.w_sum[m - 1], xi.im), s_)));
         }
         nrm += (double)abs2(y);
     }

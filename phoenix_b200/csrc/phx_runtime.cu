@@ -30,6 +30,7 @@
 #include "phx_step_fused.cuh"
 #include "phx_step_tma.cuh"
 #include "phx_rt.hpp"
+#include "phx_adjoint.cuh"
 
 namespace phx {
 
@@ -51,6 +52,9 @@ struct EngineBase {
     virtual void set_time(double t, double dt) = 0;
     virtual double sum_abs2(int field) = 0;
     virtual void field_ptr(int field, int group, void** ptr, int64_t* pitch) = 0;
+    virtual void field_device(int field, int group, void* dev, int64_t count, bool upload) = 0;
+    virtual void adjoint_forward(int64_t iterations, int64_t every) = 0;
+    virtual void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump) = 0;
 
     // ---- per-launch event timing (phx_profile_*)
     bool profiling = false;
@@ -139,6 +143,10 @@ struct Engine final : EngineBase {
 
     // simulation clock, in the build precision (SystemParameters::p.t / p.dt)
     T t = 0, dt = 0, fft_cached_t = 0;
+    // stochastic noise: Solver::iterate calls so far (the generator's counter)
+    // and dw * sqrt(dt) of the current iteration (solver.cu:36-45)
+    uint64_t noise_iteration = 0;
+    T noise_amp = 0;
     double r7_prev = 0, r7_cur = 0;  // DP45 reference norm: outer halo ring carried between steps
     int64_t accepted_steps = 0;
 
@@ -214,7 +222,7 @@ struct Engine final : EngineBase {
     // every iteration)
     bool fused_eligible_static() const {
         return P.iterator == PHX_ITER_RK4 && !P.tetm && P.n_pump_groups <= 1 && P.n_potential_groups <= 1 &&
-               P.n_pulse_groups == 0;
+               P.n_pulse_groups == 0 && !(P.stochastic_amplitude > 0.0);
     }
     long long rows_per_block(int sh) const { return (long long)kShapeRB[sh] * kShapeWarps[sh]; }
     long long grid_y(long long r0, long long r1) const {
@@ -403,7 +411,25 @@ struct Engine final : EngineBase {
         S.n_pulse = P.n_pulse_groups;
         S.dt = dt;
         S.error_passes = 1;
+        // stochastic terms of this iteration (noise drawn in the kernels)
+        S.noise.on = P.stochastic_amplitude > 0.0;
+        S.noise.key0 = (uint32_t)P.seed;
+        S.noise.key1 = (uint32_t)(P.seed >> 32);
+        S.noise.it_lo = (uint32_t)noise_iteration;
+        S.noise.it_hi = (uint32_t)(noise_iteration >> 32);
+        S.noise_amp = noise_amp;
+        S.dV = d.dV;
+        S.four_dV = (T)4.0 * d.dV;
+        S.gamma_c = (T)P.gamma_c;
+        S.noise_scale = std::sqrt((T)P.gamma_c / S.four_dV);
         return S;
+    }
+    // weight sum of a stage sum's dw term: the right fold w_1 + (w_2 + (...))
+    // of the weights the reference instantiates (kernel_summation.cuh:62-64)
+    static T right_fold(const T* w, int n) {
+        T acc = w[n - 1];
+        for (int q = n - 2; q >= 0; --q) acc = w[q] + acc;
+        return acc;
     }
 
     // temporal amplitudes at t (amp) and t+dt (amp_next): updateKernelTime
@@ -662,6 +688,8 @@ struct Engine final : EngineBase {
             S.stage = s;
             S.b = bw[s - 1];
             if (s < 4) S.dtw = dt * aw[s - 1];
+            // RK4 stage sums (runge_kutta.cu:78-91): (1/2), (0, 1/2), (0, 0, 1), (b1..b4)
+            S.w_sum = s < 4 ? aw[s - 1] : right_fold(bw, 4);
             auto wire = [this, s](StageParams<T>& X, int q) {
                 X.psi0 = cplane(psi[q]);
                 X.n0 = rplane(nres[q]);
@@ -729,6 +757,7 @@ struct Engine final : EngineBase {
             S.nw = nw[s - 1];
             for (int q = 0; q < S.nw; ++q) S.w[q] = a[s - 1][q];
             if (S.nw == 1) S.dtw = dt * a[s - 1][0];
+            S.w_sum = right_fold(S.w, S.nw);
             auto wire = [this, s, final_fixed](StageParams<T>& X, int q) {
                 X.psi0 = cplane(psi[q]);
                 X.n0 = rplane(nres[q]);
@@ -787,6 +816,17 @@ struct Engine final : EngineBase {
             std::memcpy(R.e, e, sizeof(R.e));
             R.passes = P.tetm ? 2 : 1;
             R.partials = reinterpret_cast<double*>(partials.p) + 2 * nb;
+            {
+                const StageParams<T> B = base_params(0);
+                R.noise = B.noise;
+                R.noise_amp = B.noise_amp;
+                for (int m = 0; m < 7; ++m) R.w_sum[m] = nw[m] ? right_fold(a[m], nw[m]) : (T)0;
+                R.R = B.R;
+                R.gamma_c = B.gamma_c;
+                R.four_dV = B.four_dV;
+                R.noise_scale = B.noise_scale;
+                R.n0 = P.use_reservoir ? rplane(nres[0]) : nullptr;
+            }
             dp45_ring_kernel<T><<<kRingBlocks, 256, 0, stream>>>(R);
             ++launches;
             PHX_CUDA(cudaGetLastError());
@@ -910,6 +950,7 @@ struct Engine final : EngineBase {
         const bool dp45 = P.iterator == PHX_ITER_DP45;
         while (its < max_iterations) {
             if (t >= t_max) break;
+            if (P.stochastic_amplitude > 0.0) noise_amp = (T)P.stochastic_amplitude * std::sqrt(dt);
             update_kernel_time();
             t = t + dt;
             cudaEvent_t ta = nullptr, tb = nullptr;
@@ -924,6 +965,7 @@ struct Engine final : EngineBase {
             }
             if (shape < 0) tune_record(ta, tb);
             ++its;
+            ++noise_iteration;
             if (t - fft_cached_t < fft_every) continue;
             fft_cached_t = t;
             if (have_mask[0] || have_mask[1]) {
@@ -975,6 +1017,241 @@ struct Engine final : EngineBase {
             tune_ev[sh].clear();
         }
         shape = best_sh;
+    }
+
+    // ------------------------------------------------------------ device-pointer field I/O
+    // A contiguous N_r x N_c array in device memory, in the build precision
+    // (complex fields interleaved), copied on the handle's stream; uploads
+    // rebuild the plane's ring.
+    void field_device(int field, int group, void* dev, int64_t count, bool upload) override {
+        if (!dev) fail(PHX_ERR_INVALID_ARG, "device pointer is NULL");
+        if (field == PHX_FFT_MASK_PLUS || field == PHX_FFT_MASK_MINUS) fail(PHX_ERR_UNSUPPORTED, "mask fields are host-only");
+        FieldRef f = field_ref(field, group);
+        const long long N = (long long)N_r * N_c;
+        if (count != (f.complex ? 2 * N : N)) fail(PHX_ERR_INVALID_ARG, "count does not match the field");
+        if (!upload) check_err_flag();
+        const size_t esz = f.complex ? sizeof(C) : sizeof(T);
+        char* base = reinterpret_cast<char*>(f.buf->p) + esz * (G * pitch + G + (long long)f.plane_index * plane);
+        if (upload) {
+            PHX_CUDA(cudaMemcpy2DAsync(base, esz * pitch, dev, esz * N_c, esz * N_c, N_r, cudaMemcpyDeviceToDevice, stream));
+            if (f.complex)
+                ring_fill_kernel<C><<<64, 256, 0, stream>>>(reinterpret_cast<C*>(base), N_r, N_c, pitch, G, P.periodic_x,
+                                                            P.periodic_y);
+            else
+                ring_fill_kernel<T><<<64, 256, 0, stream>>>(reinterpret_cast<T*>(base), N_r, N_c, pitch, G, P.periodic_x,
+                                                            P.periodic_y);
+            PHX_CUDA(cudaGetLastError());
+        } else {
+            PHX_CUDA(cudaMemcpy2DAsync(dev, esz * N_c, base, esz * pitch, esz * N_c, N_r, cudaMemcpyDeviceToDevice, stream));
+        }
+    }
+
+    // ------------------------------------------------------------ adjoint
+    // Forward with checkpoints every `every` iterations, then reverse sweeps
+    // segment by segment: recompute the segment's states and stage values
+    // Y2..Y4 with the stage kernels (bit-identical to the forward), then run
+    // the four vector-Jacobian stage kernels of phx_adjoint.cuh per
+    // iteration, last to first.
+    std::vector<std::unique_ptr<DevBuf>> ck_psi, ck_n;    // checkpoints (state planes)
+    std::vector<std::unique_ptr<DevBuf>> sg_psi, sg_n;    // states of one segment
+    std::vector<std::unique_ptr<DevBuf>> st_psi, st_n;    // Y2..Y4 of every iteration of a segment
+    DevBuf lam_psi[2], lam_n[2], yb_psi[2], yb_n[2], la_psi, la_n, pbar;
+    int64_t adj_T = 0, adj_every = 0;
+    T adj_dt = 0;
+    bool adj_ready = false;
+
+    void adjoint_check() {
+        if (P.iterator != PHX_ITER_RK4 || P.tetm) fail(PHX_ERR_UNSUPPORTED, "the adjoint covers scalar fixed-step RK4");
+        if (!P.periodic_x || !P.periodic_y) fail(PHX_ERR_UNSUPPORTED, "the adjoint needs periodic boundaries on both axes");
+        if (P.stochastic_amplitude > 0.0) fail(PHX_ERR_UNSUPPORTED, "the adjoint of a noisy run is not defined here");
+        if (have_mask[0] || have_mask[1]) fail(PHX_ERR_UNSUPPORTED, "the adjoint does not cover the k-space filter");
+        if (P.n_pump_groups > 1 || P.n_potential_groups > 1 || P.n_pulse_groups != 0)
+            fail(PHX_ERR_UNSUPPORTED, "the adjoint takes at most one pump and one potential group and no pulse");
+        for (int g = 0; g < P.n_pump_groups; ++g)
+            if (pump_t[g].kind != PHX_TEMPORAL_CONSTANT) fail(PHX_ERR_UNSUPPORTED, "the adjoint needs constant envelopes");
+        for (int g = 0; g < P.n_potential_groups; ++g)
+            if (pot_t[g].kind != PHX_TEMPORAL_CONSTANT) fail(PHX_ERR_UNSUPPORTED, "the adjoint needs constant envelopes");
+    }
+    void plane_copy(DevBuf& dst, const DevBuf& src) {
+        PHX_CUDA(cudaMemcpyAsync(dst.p, src.p, src.bytes, cudaMemcpyDeviceToDevice, stream));
+    }
+    void ensure_planes(std::vector<std::unique_ptr<DevBuf>>& v, size_t n, size_t bytes) {
+        while (v.size() < n) {
+            v.emplace_back(new DevBuf());
+            v.back()->alloc(bytes, stream);
+        }
+    }
+    void adjoint_forward(int64_t iterations, int64_t every) override {
+        adjoint_check();
+        if (iterations < 1) fail(PHX_ERR_INVALID_ARG, "iterations must be >= 1");
+        if (every <= 0) every = (int64_t)std::ceil(std::sqrt((double)iterations));
+        if (every > iterations) every = iterations;
+        const int64_t nck = (iterations + every - 1) / every;
+        const size_t cb = sizeof(C) * plane, rb = sizeof(T) * plane;
+        ensure_planes(ck_psi, (size_t)nck, cb);
+        if (P.use_reservoir) ensure_planes(ck_n, (size_t)nck, rb);
+        adj_ready = false;
+        for (int64_t k = 0; k < nck; ++k) {
+            plane_copy(*ck_psi[k], psi[0]);
+            if (P.use_reservoir) plane_copy(*ck_n[k], nres[0]);
+            const int64_t len = std::min(every, iterations - k * every);
+            phx_step_info info{};
+            step(len, &info);
+            if (info.iterations != len) fail(PHX_ERR_STATE, "t_max was reached inside the adjoint's forward run");
+        }
+        adj_T = iterations;
+        adj_every = every;
+        adj_dt = dt;
+        adj_ready = true;
+    }
+    // one RK4 iteration with the stage kernels: state (yp, yn) -> (op, on),
+    // stage values Y2..Y4 into (sp[0..2], sn[0..2])
+    void rk4_recompute(DevBuf& yp, DevBuf* yn, DevBuf* sp[3], DevBuf* sn[3], DevBuf& op, DevBuf* on) {
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
+        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
+        for (int s = 1; s <= 4; ++s) {
+            StageParams<T> S = base_params(0);
+            set_coefficients(S, cw[s - 1]);
+            region(S, 4 - s);
+            S.stage = s;
+            S.b = bw[s - 1];
+            if (s < 4) S.dtw = dt * aw[s - 1];
+            auto wire = [&, s](StageParams<T>& X, int) {
+                X.psi0 = cplane(yp);
+                X.n0 = yn ? rplane(*yn) : nullptr;
+                X.psi_in = s == 1 ? cplane(yp) : cplane(*sp[s - 2]);
+                X.n_in = s == 1 ? (yn ? rplane(*yn) : nullptr) : (sn[s - 2] ? rplane(*sn[s - 2]) : nullptr);
+                X.psi_out = s == 4 ? cplane(op) : cplane(*sp[s - 1]);
+                X.n_out = s == 4 ? (on ? rplane(*on) : nullptr) : (sn[s - 1] ? rplane(*sn[s - 1]) : nullptr);
+                X.acc_psi = cplane(acc_psi[0]);
+                X.acc_n = rplane(acc_n[0]);
+                X.pump = rplane(pump[0]);
+                X.pot = rplane(pot[0]);
+                X.pulse = cplane(pulse[0]);
+            };
+            if (s == 1)
+                launch<kRk4First>(S, wire);
+            else if (s < 4)
+                launch<kRk4Mid>(S, wire);
+            else
+                launch<kRk4Last>(S, wire);
+        }
+    }
+    void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump) override {
+        if (!adj_ready) fail(PHX_ERR_STATE, "phx_adjoint_forward must run first");
+        if (!dpsi) fail(PHX_ERR_INVALID_ARG, "dL/dpsi_T is NULL");
+        adjoint_check();
+        const bool res = P.use_reservoir != 0;
+        const size_t cb = sizeof(C) * plane, rb = sizeof(T) * plane;
+        const int64_t every = adj_every, nck = (adj_T + every - 1) / every;
+        ensure_planes(sg_psi, (size_t)every + 1, cb);
+        ensure_planes(st_psi, (size_t)(3 * every), cb);
+        if (res) {
+            ensure_planes(sg_n, (size_t)every + 1, rb);
+            ensure_planes(st_n, (size_t)(3 * every), rb);
+        }
+        for (int b = 0; b < 2; ++b) {
+            if (!lam_psi[b].p) lam_psi[b].alloc(cb, stream);
+            if (!yb_psi[b].p) yb_psi[b].alloc(cb, stream);
+            if (res && !lam_n[b].p) lam_n[b].alloc(rb, stream);
+            if (res && !yb_n[b].p) yb_n[b].alloc(rb, stream);
+        }
+        if (!la_psi.p) la_psi.alloc(cb, stream);
+        if (res && !la_n.p) la_n.alloc(rb, stream);
+        if (!pbar.p) pbar.alloc(rb, stream);
+        PHX_CUDA(cudaMemsetAsync(pbar.p, 0, rb, stream));
+        // lam_T = dL/d(psi_T, n_T), with periodic images
+        int cur = 0;
+        unpack_interior_kernel<C><<<256, 256, 0, stream>>>(static_cast<const C*>(dpsi), cplane(lam_psi[0]), pitch, N_r, N_c);
+        ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(lam_psi[0]), N_r, N_c, pitch, G, 1, 1);
+        if (res) {
+            if (dn)
+                unpack_interior_kernel<T><<<256, 256, 0, stream>>>(static_cast<const T*>(dn), rplane(lam_n[0]), pitch, N_r, N_c);
+            else
+                PHX_CUDA(cudaMemsetAsync(lam_n[0].p, 0, rb, stream));
+            ring_fill_kernel<T><<<64, 256, 0, stream>>>(rplane(lam_n[0]), N_r, N_c, pitch, G, 1, 1);
+        }
+        PHX_CUDA(cudaGetLastError());
+        const T saved_dt = dt;
+        dt = adj_dt;
+        DevBuf scratch_psi, scratch_n;  // the recomputed state after a segment's last iteration is not needed
+        scratch_psi.alloc(cb, stream);
+        if (res) scratch_n.alloc(rb, stream);
+        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
+        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        for (int64_t k = nck - 1; k >= 0; --k) {
+            const int64_t len = std::min(every, adj_T - k * every);
+            plane_copy(*sg_psi[0], *ck_psi[k]);
+            if (res) plane_copy(*sg_n[0], *ck_n[k]);
+            for (int64_t j = 0; j < len; ++j) {
+                DevBuf* sp[3] = {st_psi[3 * j].get(), st_psi[3 * j + 1].get(), st_psi[3 * j + 2].get()};
+                DevBuf* sn[3] = {res ? st_n[3 * j].get() : nullptr, res ? st_n[3 * j + 1].get() : nullptr,
+                                 res ? st_n[3 * j + 2].get() : nullptr};
+                DevBuf& op = j + 1 < len ? *sg_psi[j + 1] : scratch_psi;
+                DevBuf* on = res ? (j + 1 < len ? sg_n[j + 1].get() : &scratch_n) : nullptr;
+                rk4_recompute(*sg_psi[j], res ? sg_n[j].get() : nullptr, sp, sn, op, on);
+            }
+            for (int64_t j = len - 1; j >= 0; --j) {
+                for (int s = 4; s >= 1; --s) {
+                    AdjParams<T> Q;
+                    std::memset(&Q, 0, sizeof(Q));
+                    Q.N_r = N_r;
+                    Q.N_c = N_c;
+                    Q.pitch = pitch;
+                    Q.Ypsi = s == 1 ? cplane(*sg_psi[j]) : cplane(*st_psi[3 * j + s - 2]);
+                    Q.Yn = res ? (s == 1 ? rplane(*sg_n[j]) : rplane(*st_n[3 * j + s - 2])) : nullptr;
+                    Q.lam_psi = cplane(lam_psi[cur]);
+                    Q.lam_n = res ? rplane(lam_n[cur]) : nullptr;
+                    Q.ybar_in_psi = cplane(yb_psi[(s + 1) & 1]);
+                    Q.ybar_in_n = res ? rplane(yb_n[(s + 1) & 1]) : nullptr;
+                    Q.ybar_out_psi = cplane(yb_psi[s & 1]);
+                    Q.ybar_out_n = res ? rplane(yb_n[s & 1]) : nullptr;
+                    Q.acc_in_psi = cplane(la_psi);
+                    Q.acc_in_n = res ? rplane(la_n) : nullptr;
+                    Q.acc_psi = s == 1 ? cplane(lam_psi[cur ^ 1]) : cplane(la_psi);
+                    Q.acc_n = res ? (s == 1 ? rplane(lam_n[cur ^ 1]) : rplane(la_n)) : nullptr;
+                    Q.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
+                    Q.pump = P.n_pump_groups ? rplane(pump[0]) : nullptr;
+                    Q.pbar = (res && P.n_pump_groups) ? rplane(pbar) : nullptr;
+                    Q.c_pot = P.n_potential_groups ? interp<T>(amp_pot[0], next_pot[0], cw[s - 1]).real() : (T)0;
+                    Q.c_pump = P.n_pump_groups ? interp<T>(amp_pump[0], next_pump[0], cw[s - 1]).real() : (T)0;
+                    Q.dt_b = adj_dt * bw[s - 1];
+                    Q.a_dt = s < 4 ? aw[s - 1] * adj_dt : (T)0;
+                    Q.A = d.ohb * d.meff;
+                    Q.ohb = d.ohb;
+                    Q.ohb_gc = d.ohb * (T)P.g_c;
+                    Q.ohb_gr = d.ohb * (T)P.g_r;
+                    Q.half_R = (T)0.5 * (T)P.R;
+                    Q.half_gamma_c = (T)0.5 * (T)P.gamma_c;
+                    Q.gamma_r = (T)P.gamma_r;
+                    Q.R = (T)P.R;
+                    Q.m2 = d.m2;
+                    Q.odx2 = d.odx2;
+                    Q.ody2 = d.ody2;
+                    Q.s = s;
+                    Q.res = res;
+                    dim3 grid((unsigned)((N_c + 31) / 32), (unsigned)((N_r + 7) / 8));
+                    cudaEvent_t a = nullptr;
+                    prof_begin(a);
+                    adj_stage_kernel<T><<<grid, 256, 0, stream>>>(Q);
+                    prof_end(PHX_KERNEL_OTHER, a, (double)N_r * N_c * (4.0 * sizeof(C) + 4.0 * sizeof(T)));
+                    ++launches;
+                    PHX_CUDA(cudaGetLastError());
+                }
+                cur ^= 1;
+            }
+        }
+        dt = saved_dt;
+        if (dpsi0) pack_interior_kernel<C><<<256, 256, 0, stream>>>(cplane(lam_psi[cur]), pitch, N_r, N_c, static_cast<C*>(dpsi0));
+        if (dn0 && res) pack_interior_kernel<T><<<256, 256, 0, stream>>>(rplane(lam_n[cur]), pitch, N_r, N_c, static_cast<T*>(dn0));
+        if (dpump) {
+            if (!(res && P.n_pump_groups)) fail(PHX_ERR_INVALID_ARG, "dL/dP needs a pump group and the reservoir");
+            pack_interior_kernel<T><<<256, 256, 0, stream>>>(rplane(pbar), pitch, N_r, N_c, static_cast<T*>(dpump));
+        }
+        PHX_CUDA(cudaGetLastError());
+        PHX_CUDA(cudaStreamSynchronize(stream));  // scratch planes are freed on return
     }
 
     double sum_abs2(int field) override {
@@ -1045,7 +1322,7 @@ void validate(const phx_params& p) {
         fail(PHX_ERR_INVALID_ARG, "temporal group count out of range (0..8)");
     if (p.n_pump_groups > 0 && !p.use_reservoir) fail(PHX_ERR_INVALID_ARG, "pump groups need use_reservoir");
     if (p.tetm && !p.use_reservoir) fail(PHX_ERR_UNSUPPORTED, "TE/TM mode reads the reservoir; set use_reservoir");
-    if (p.stochastic_amplitude != 0.0) fail(PHX_ERR_UNSUPPORTED, "stochastic noise is not available in this build");
+    if (!std::isfinite(p.stochastic_amplitude)) fail(PHX_ERR_INVALID_ARG, "stochastic_amplitude must be finite");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         (void)cudaGetLastError();
@@ -1159,6 +1436,27 @@ phx_status phx_sum_abs2(phx_handle* h, int32_t field, double* out) {
 phx_status phx_field_device_ptr(phx_handle* h, int32_t field, int32_t group, void** dev_ptr, int64_t* row_pitch_elems) {
     if (!h || !dev_ptr) return PHX_ERR_INVALID_ARG;
     return guard(h, [&] { h->eng->field_ptr(field, group, dev_ptr, row_pitch_elems); });
+}
+
+phx_status phx_set_field_device(phx_handle* h, int32_t field, int32_t group, const void* dev, int64_t count) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->field_device(field, group, const_cast<void*>(dev), count, true); });
+}
+
+phx_status phx_get_field_device(phx_handle* h, int32_t field, int32_t group, void* dev, int64_t count) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->field_device(field, group, dev, count, false); });
+}
+
+phx_status phx_adjoint_forward(phx_handle* h, int64_t iterations, int64_t checkpoint_every) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->adjoint_forward(iterations, checkpoint_every); });
+}
+
+phx_status phx_adjoint_backward(phx_handle* h, const void* dpsi_T, const void* dn_T, void* dpsi_0, void* dn_0,
+                                void* dpump) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] { h->eng->adjoint_backward(dpsi_T, dn_T, dpsi_0, dn_0, dpump); });
 }
 
 phx_status phx_profile_enable(phx_handle* h, int32_t enable) {

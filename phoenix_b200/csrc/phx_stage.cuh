@@ -14,6 +14,7 @@
 #pragma once
 
 #include "phx_device.cuh"
+#include "phx_noise.cuh"
 
 namespace phx {
 
@@ -69,6 +70,14 @@ struct StageParams {
     T dt;
     double* partials;    // kStackError: per-block (error, norm) pairs
     int error_passes;    // 1, or 2 for the TE/TM double count
+    // stochastic terms (noise.on): drift in the right-hand side, dw in the
+    // stage sums (kernel_summation.cuh:216-224)
+    NoiseParams noise;
+    T noise_amp;         // dw * sqrt(dt) of this iteration
+    T w_sum;             // right fold of this stage sum's weights
+    T dV, four_dV;       // dV, 4 dV
+    T gamma_c;
+    T noise_scale;       // sqrt(gamma_c / (4 dV)), the scale without reservoir
 };
 
 // ---- 16-byte packs: CPT grid points per lane ----
@@ -136,6 +145,13 @@ __device__ __forceinline__ cx<T> shfl_dn1(cx<T> z) {
 // real (checked on the host), so every reservoir expression below is the
 // reference's complex one with a zero imaginary part carried exactly.
 
+// (one_over_h_bar_s g_c) (-i psi) / dV: the stochastic drift of psi
+template <typename T>
+__device__ __forceinline__ cx<T> noise_drift(const StageParams<T>& P, cx<T> in_wf_mi) {
+    const cx<T> d = smul(P.ohb_gc, in_wf_mi);
+    return mk(rdiv(d.re, P.dV), rdiv(d.im, P.dV));
+}
+
 // Right-hand side of gp_scalar, scalar branch, one grid point.
 template <typename T, bool RES>
 __device__ __forceinline__ void rhs_scalar(const StageParams<T>& P, long long idx, cx<T> in_wf, cx<T> up, cx<T> dn,
@@ -165,7 +181,23 @@ __device__ __forceinline__ void rhs_scalar(const StageParams<T>& P, long long id
         const cx<T> pulse = ld1(P.pulse + idx + g * P.plane);
         wf = cadd(wf, cmul(smul(P.ohb, pulse), P.pulse_c[g]));
     }
+    if (P.noise.on) {
+        // stochastic drift (kernel_gp_compute.cuh:82-84, 101-103)
+        wf = csub(wf, noise_drift(P, in_wf_mi));
+        if constexpr (RES) k_rv = radd(k_rv, rdiv(rmul(P.R, in_rv), P.dV));
+    }
     k_wf = wf;
+}
+
+// dw term of a stage sum at interior point (r, c): w_sum * xi * sqrt((R n0 +
+// gamma_c) / (4 dV)) with n0 the state reservoir (kernel_summation.cuh:216-224);
+// the reference's product with the complex square root (x, 0) keeps each
+// component's two roundings
+template <typename T, bool RES>
+__device__ __forceinline__ cx<T> stage_noise(const StageParams<T>& P, int r, int c, T n0) {
+    const cx<T> xi = noise_xi(P.noise, noise_point(r, c, P.N_r, P.N_c, P.img_x, P.img_y), P.noise_amp);
+    const T sc = RES ? rsqrt_rn(rdiv(radd(rmul(P.R, n0), P.gamma_c), P.four_dV)) : P.noise_scale;
+    return mk(rmul(rmul(P.w_sum, xi.re), sc), rmul(rmul(P.w_sum, xi.im), sc));
 }
 
 // Periodic images of a produced point (wavefunction and reservoir): every
@@ -288,6 +320,11 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
                             if constexpr (RES)
                                 out_rv.v[j] = radd(n0.v[j], rmul(P.dt, radd(accn.v[j], rmul(P.b, out_rv.v[j]))));
                         }
+                        if (P.noise.on) {
+                            T nn = (T)0;
+                            if constexpr (RES) nn = n0.v[j];
+                            out_wf.v[j] = cadd(out_wf.v[j], stage_noise<T, RES>(P, r, c + j, nn));
+                        }
                     }
                     if constexpr (KIND != kRk4Last) {
                         stp(P.acc_psi + idx, acc);
@@ -347,6 +384,11 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
                                 }
                                 out_wf.v[j] = cadd(y0.v[j], smul(P.dt, a));
                                 if constexpr (RES) out_rv.v[j] = radd(n0.v[j], rmul(P.dt, an));
+                            }
+                            if (P.noise.on) {
+                                T nn = (T)0;
+                                if constexpr (RES) nn = n0.v[j];
+                                out_wf.v[j] = cadd(out_wf.v[j], stage_noise<T, RES>(P, r, c + j, nn));
                             }
                         }
                     }

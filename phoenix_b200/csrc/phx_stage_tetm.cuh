@@ -109,10 +109,12 @@ __device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, 
     res = cadd(res, smul(rmul(Q.ohb_gpm, nmi), in_wf_plus_mi));
     res = cadd(res, smul(Q.ohb_dlt, hcp));
     for (int g = 0; g < P.n_pulse; ++g) res = cadd(res, cmul(smul(P.ohb, ld1(P.pulse + idx + g * P.plane)), P.pulse_c[g]));
+    if (P.noise.on) res = csub(res, noise_drift(P, in_wf_plus_mi));
     kwp = res;
     // reservoir plus
     T r = rmul(-radd(P.gamma_r, rmul(P.R, npl)), rvp);
     for (int g = 0; g < P.n_pump; ++g) r = radd(r, rmul(__ldg(P.pump + idx + g * P.plane), P.pump_c[g].re));
+    if (P.noise.on) r = radd(r, rdiv(rmul(P.R, rvp), P.dV));
     krp = r;
     // wavefunction minus
     res = smul(Q.ohb_meff, hrm);
@@ -127,10 +129,12 @@ __device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, 
     res = cadd(res, smul(rmul(Q.ohb_gpm, npl), in_wf_minus_mi));
     res = cadd(res, smul(Q.ohb_dlt, hcm));
     for (int g = 0; g < P.n_pulse; ++g) res = cadd(res, cmul(smul(P.ohb, ld1(Q.pulse + idx + g * P.plane)), P.pulse_c[g]));
+    if (P.noise.on) res = csub(res, noise_drift(P, in_wf_minus_mi));
     kwm = res;
     // reservoir minus
     r = rmul(-radd(P.gamma_r, rmul(P.R, nmi)), rvm);
     for (int g = 0; g < P.n_pump; ++g) r = radd(r, rmul(__ldg(Q.pump + idx + g * P.plane), P.pump_c[g].re));
+    if (P.noise.on) r = radd(r, rdiv(rmul(P.R, rvm), P.dV));
     krm = r;
 }
 
@@ -218,6 +222,15 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                             orp.v[j] = radd(n0p.v[j], rmul(P.dt, radd(anp.v[j], rmul(P.b, orp.v[j]))));
                             orm.v[j] = radd(n0m.v[j], rmul(P.dt, radd(anm.v[j], rmul(P.b, orm.v[j]))));
                         }
+                        if (P.noise.on) {
+                            // one noise value for both polarisations, scaled by the plus
+                            // reservoir; the final sum updates n+ in place before the minus
+                            // wavefunction's sum runs (cuda_macro.cuh:200-229), so psi- sees
+                            // the new n+ there
+                            owp.v[j] = cadd(owp.v[j], stage_noise<T, true>(P, r, c + j, n0p.v[j]));
+                            owm.v[j] = cadd(owm.v[j],
+                                            stage_noise<T, true>(P, r, c + j, KIND == kRk4Last ? orp.v[j] : n0p.v[j]));
+                        }
                     }
                     if constexpr (KIND != kRk4Last) {
                         stp(P.acc_psi + idx, ap);
@@ -282,6 +295,11 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                                 owm.v[j] = cadd(y0m.v[j], smul(P.dt, a2));
                                 orp.v[j] = radd(n0p.v[j], rmul(P.dt, b1));
                                 orm.v[j] = radd(n0m.v[j], rmul(P.dt, b2));
+                            }
+                            if (P.noise.on) {
+                                owp.v[j] = cadd(owp.v[j], stage_noise<T, true>(P, r, c + j, n0p.v[j]));
+                                owm.v[j] = cadd(owm.v[j], stage_noise<T, true>(P, r, c + j,
+                                                                               KIND == kStackFinal ? orp.v[j] : n0p.v[j]));
                             }
                         }
                     }

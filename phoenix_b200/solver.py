@@ -62,6 +62,8 @@ class SystemParameters:
     potential_temporal: List[Temporal] = field(default_factory=list)
     pulse_temporal: List[Temporal] = field(default_factory=list)
     norm_mode: str = "reference"  # DP45 error norm: "reference" (halo-padded sums) or "interior"
+    stochastic_amplitude: float = 0.0  # --dw; noise is on when > 0
+    random_seed: int = 0  # key of the counter-based noise generator
     device: int = 0
 
     def magic_timestep(self) -> float:
@@ -92,7 +94,8 @@ class SystemParameters:
         p.t0, p.t_max = float(self.t0), float(self.t_max)
         p.tol, p.dt_min, p.dt_max = float(self.tolerance), float(self.dt_min), float(self.dt_max)
         p.fft_every = float(self.fft_every)
-        p.stochastic_amplitude = 0.0
+        p.stochastic_amplitude = float(self.stochastic_amplitude)
+        p.seed = int(self.random_seed) & 0xFFFFFFFFFFFFFFFF
         p.n_pump_groups = len(self.pump_temporal)
         p.n_potential_groups = len(self.potential_temporal)
         p.n_pulse_groups = len(self.pulse_temporal)
@@ -172,6 +175,78 @@ class Solver:
         view = out.view(rtype)
         L.check(self._lib.phx_get_field(self._h, fid, group, view.ctypes.data_as(C.c_void_p), view.size, code), self._h)
         return out
+
+    # -- device tensors (torch), no host round trip
+    def _check_tensor(self, name, t):
+        import torch
+
+        cplx = name in L.COMPLEX_FIELDS
+        f32 = self.system.dtype not in ("f64", "fp64", "double")
+        want = (torch.complex64 if f32 else torch.complex128) if cplx else (torch.float32 if f32 else torch.float64)
+        if t.dtype != want or tuple(t.shape) != self._shape() or not t.is_contiguous() or not t.is_cuda:
+            raise ValueError(f"{name}: expected a contiguous CUDA {want} tensor of shape {self._shape()}")
+        return (2 if cplx else 1) * t.numel()
+
+    def _order_after_torch(self):
+        import torch
+
+        s = torch.cuda.ExternalStream(self.stream)
+        s.wait_stream(torch.cuda.current_stream())
+
+    def _order_torch_after(self):
+        import torch
+
+        torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(self.stream))
+
+    def set_field_tensor(self, name: str, tensor, group: int = 0):
+        """Upload from a torch CUDA tensor (build precision, C-contiguous)."""
+        n = self._check_tensor(name, tensor)
+        self._order_after_torch()
+        L.check(self._lib.phx_set_field_device(self._h, L.FIELDS[name], group, C.c_void_p(tensor.data_ptr()), n),
+                self._h)
+
+    def get_field_tensor(self, name: str, group: int = 0, out=None):
+        """Download into a torch CUDA tensor (allocated when `out` is None)."""
+        import torch
+
+        cplx = name in L.COMPLEX_FIELDS
+        f32 = self.system.dtype not in ("f64", "fp64", "double")
+        dt = (torch.complex64 if f32 else torch.complex128) if cplx else (torch.float32 if f32 else torch.float64)
+        if out is None:
+            out = torch.empty(self._shape(), dtype=dt, device=f"cuda:{self.system.device}")
+        n = self._check_tensor(name, out)
+        self._order_after_torch()
+        L.check(self._lib.phx_get_field_device(self._h, L.FIELDS[name], group, C.c_void_p(out.data_ptr()), n),
+                self._h)
+        self._order_torch_after()
+        return out
+
+    # -- adjoint
+    def adjoint_forward(self, iterations: int, checkpoint_every: int = 0):
+        """Run `iterations` RK4 iterations keeping checkpoints (default every ceil(sqrt(iterations)))."""
+        self._order_after_torch()
+        L.check(self._lib.phx_adjoint_forward(self._h, C.c_int64(iterations), C.c_int64(checkpoint_every)), self._h)
+        self._order_torch_after()
+
+    def adjoint_backward(self, dpsi_T, dn_T=None, want_psi0=True, want_n0=True, want_pump=True):
+        """dL/d(final state) -> (dL/dpsi_0, dL/dn_0, dL/dP) as torch CUDA tensors (None where not wanted)."""
+        import torch
+
+        f32 = self.system.dtype not in ("f64", "fp64", "double")
+        cdt, rdt = (torch.complex64, torch.float32) if f32 else (torch.complex128, torch.float64)
+        dev = dpsi_T.device
+        self._check_tensor("psi_plus", dpsi_T)
+        if dn_T is not None:
+            self._check_tensor("n_plus", dn_T)
+        g_psi = torch.empty(self._shape(), dtype=cdt, device=dev) if want_psi0 else None
+        g_n = torch.empty(self._shape(), dtype=rdt, device=dev) if want_n0 and self.system.use_reservoir else None
+        g_p = torch.empty(self._shape(), dtype=rdt, device=dev) if want_pump else None
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+        self._order_after_torch()
+        L.check(self._lib.phx_adjoint_backward(self._h, ptr(dpsi_T), ptr(dn_T), ptr(g_psi), ptr(g_n), ptr(g_p)),
+                self._h)
+        self._order_torch_after()
+        return g_psi, g_n, g_p
 
     # -- time
     @property
@@ -275,6 +350,7 @@ def system_from_case(case: dict, **overrides) -> SystemParameters:
         use_adaptive_timestep=bool(case.get("adaptive", 0)), tolerance=case.get("tol", 0.1),
         dt_min=case.get("dt_min", 1e-4), dt_max=case.get("dt_max", 3.0), fft_every=case.get("fft_every", 1e9),
         t0=case.get("t0", 0.0), t_max=case["t_max"], dt=case["dt"],
+        stochastic_amplitude=case.get("dw", 0.0), random_seed=case.get("seed", 0),
         pump_temporal=temporal(case.get("pump_t"), npump),
         potential_temporal=temporal(case.get("potential_t"), len(case.get("potentials", []))),
         pulse_temporal=temporal(case.get("pulse_t"), len(case.get("pulses", []))))
