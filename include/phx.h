@@ -53,7 +53,29 @@ typedef enum {
 typedef enum { PHX_F32 = 0, PHX_F64 = 1 } phx_dtype;
 
 /* iterator keys of REGISTER_SOLVER: "RK4" (runge_kutta.cu:96), "DP45" (dormand_prince.cu:97) */
-typedef enum { PHX_ITER_RK4 = 0, PHX_ITER_DP45 = 1 } phx_iterator;
+/* REGISTER_SOLVER keys of the reference (source/cuda_solver/solver/iterator/*.cu) */
+typedef enum {
+    PHX_ITER_RK4 = 0,       /* "RK4"      runge_kutta.cu:96 */
+    PHX_ITER_DP45 = 1,      /* "DP45"     dormand_prince.cu:97 (adaptive) */
+    PHX_ITER_RK3 = 2,       /* "RK3"      runge_kutta.cu:51 */
+    PHX_ITER_SSPRK3 = 3,    /* "SSPRK3"   SSPRK3.cu:45 */
+    PHX_ITER_MP = 4,        /* "MP"       explicit_mp.cu:42 */
+    PHX_ITER_HEUN2 = 5,     /* "Heun2"    heun.cu:45 */
+    PHX_ITER_HEUN3 = 6,     /* "Heun3"    heun.cu:84 */
+    PHX_ITER_HW = 7,        /* "HW"       houwen_wray.cu:45 */
+    PHX_ITER_NEWTON = 8,    /* "Newton"   newton.cu:36 (explicit Euler) */
+    PHX_ITER_NYSTROEM = 9,  /* "Nystroem" nystroem.cu:60 */
+    PHX_ITER_RALSTON = 10,  /* "Ralston"  ralston.cu:45 */
+    PHX_ITER_RALSTON3 = 11, /* "Ralston3" ralston.cu:84 */
+    PHX_ITER_RALSTON4 = 12, /* "Ralston4" ralston.cu:128 */
+    PHX_ITER_RULE38 = 13,   /* "Rule38"   rule38.cu:51 */
+    PHX_ITER_BOSHA = 14,    /* "BoSha"     bogacki.cu:78 (adaptive) */
+    PHX_ITER_CASHKARP = 15, /* "CashKarp"  cash_karp.cu:86 (adaptive) */
+    PHX_ITER_FEHLBERG2 = 16,/* "Fehlberg2" fehlberg.cu:75 (adaptive) */
+    PHX_ITER_FEHLBERG5 = 17,/* "Fehlberg5" fehlberg.cu:155 (adaptive) */
+    PHX_ITER_DP85 = 18,     /* "DP85"      dormand_prince.cu:206 (adaptive) */
+    PHX_ITER_NSRK78 = 19    /* "NSRK78"    NSRK78.cu:119 (adaptive) */
+} phx_iterator;
 
 /* DP45 error norm.  PHX_NORM_REFERENCE reproduces the reference's sums over
  * halo-padded subgrids of a single subgrid (cuda_matrix.cuh:614-632,699-705,

@@ -49,7 +49,7 @@ static void dft2d_f32(float* buf, int n0, int n1, int sign) {
  *   Box-Muller (1958): z0 = r cos(2 pi u2), z1 = r sin(2 pi u2),
  *   r = sqrt(-2 ln u1), with ln, cos and sin evaluated by the series below
  *   in float, each operation rounded on its own (no contraction).
- * The point id numbers the padded coordinates (row + 8) (N_c + 16) + col + 8
+ * The point id numbers the padded coordinates (row + 16) (N_c + 32) + col + 16
  * after wrapping periodic axes, so periodic images draw their point's value. */
 static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
     for (int round = 0; round < 10; ++round) {

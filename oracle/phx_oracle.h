@@ -12,6 +12,11 @@
  *   Solver::updateKernelTime  source/cuda_solver/solver/iterator/solver_iterator.cu:11-28
  *   RungeKutta4::step         source/cuda_solver/solver/iterator/runge_kutta.cu:74-94
  *   DormandPrince45::step     source/cuda_solver/solver/iterator/dormand_prince.cu:37-95
+ *   the fixed-step tableaux   runge_kutta.cu:33-47 (RK3), SSPRK3.cu:27-41, explicit_mp.cu:28-38,
+ *                             heun.cu:31-41,66-80, houwen_wray.cu:27-41, newton.cu:24-30,
+ *                             nystroem.cu:30-56, ralston.cu:31-41,66-80,106-124, rule38.cu:28-47
+ *   the adaptive tableaux     bogacki.cu:27-76, cash_karp.cu:31-84, fehlberg.cu:33-73,100-153,
+ *                             dormand_prince.cu:128-204, NSRK78.cu:37-117
  *   gp_scalar                 include/kernel/kernel_gp_compute.cuh:18-236
  *   runge_sum_to_input_k / runge_add_to_input_k / runge_sum_to_error
  *                             include/kernel/kernel_summation.cuh:66-289
@@ -37,7 +42,14 @@
 extern "C" {
 #endif
 
-enum { PHX_ORACLE_RK4 = 0, PHX_ORACLE_DP45 = 1 };
+/* iterator keys: the reference's REGISTER_SOLVER names, numbered as in include/phx.h */
+enum {
+    PHX_ORACLE_RK4 = 0, PHX_ORACLE_DP45 = 1, PHX_ORACLE_RK3 = 2, PHX_ORACLE_SSPRK3 = 3, PHX_ORACLE_MP = 4,
+    PHX_ORACLE_HEUN2 = 5, PHX_ORACLE_HEUN3 = 6, PHX_ORACLE_HW = 7, PHX_ORACLE_NEWTON = 8, PHX_ORACLE_NYSTROEM = 9,
+    PHX_ORACLE_RALSTON = 10, PHX_ORACLE_RALSTON3 = 11, PHX_ORACLE_RALSTON4 = 12, PHX_ORACLE_RULE38 = 13,
+    PHX_ORACLE_BOSHA = 14, PHX_ORACLE_CASHKARP = 15, PHX_ORACLE_FEHLBERG2 = 16, PHX_ORACLE_FEHLBERG5 = 17,
+    PHX_ORACLE_DP85 = 18, PHX_ORACLE_NSRK78 = 19
+};
 enum { PHX_ORACLE_T_CONSTANT = 0, PHX_ORACLE_T_IEXP = 1, PHX_ORACLE_T_COS = 2, PHX_ORACLE_T_GAUSS = 3 };
 
 #define PHX_ORACLE_MAX_GROUPS 8
@@ -55,7 +67,7 @@ typedef struct {
     int32_t periodic_x, periodic_y;
     int32_t tetm;
     int32_t use_reservoir;
-    int32_t iterator; /* PHX_ORACLE_RK4 / PHX_ORACLE_DP45 */
+    int32_t iterator; /* PHX_ORACLE_* */
     int32_t adaptive; /* DP45 only */
     double dt, t0, t_max;
     double tol, dt_min, dt_max;

@@ -20,6 +20,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libphx_oracle.so")
 MAX_GROUPS = 8
 TEMPORAL = {"constant": 0, "iexp": 1, "osc": 1, "cos": 2, "gauss": 3}
+# REGISTER_SOLVER keys of the reference, numbered as in include/phx.h
+ITERATORS = {"RK4": 0, "DP45": 1, "RK3": 2, "SSPRK3": 3, "MP": 4, "HEUN2": 5, "HEUN3": 6, "HW": 7, "NEWTON": 8,
+             "NYSTROEM": 9, "RALSTON": 10, "RALSTON3": 11, "RALSTON4": 12, "RULE38": 13, "BOSHA": 14,
+             "CASHKARP": 15, "FEHLBERG2": 16, "FEHLBERG5": 17, "DP85": 18, "NSRK78": 19}
 
 
 class Temporal(C.Structure):
@@ -94,7 +98,7 @@ def make_params(case):
     p.tetm = int(case.get("tetm", 0))
     npump = len(case.get("pumps", []))
     p.use_reservoir = int(npump > 0 or bool(case.get("n0_amp", 0.0)))
-    p.iterator = 1 if case["iterator"].upper() == "DP45" else 0
+    p.iterator = ITERATORS[case["iterator"].upper()]
     p.adaptive = int(case.get("adaptive", 0))
     p.use_fft_mask = int(bool(case.get("mask_cut")))
     p.stochastic_amplitude = float(case.get("dw", 0.0))

@@ -63,8 +63,8 @@ __device__ __forceinline__ cx<T> cmul_general(cx<T> s, cx<T> z) { return cmul(s,
 // points at interior (0, 0); rows and columns -G .. N+G-1 are addressable.
 // The ring holds zeros along non-periodic axes and periodic images of the
 // first/last interior row/column along periodic axes.
-constexpr int kRing = 8;           // G: ring width (>= stages of RK4 / DP45)
+constexpr int kRing = 8;           // G: ring width of RK4 / DP45 handles (wider for larger halos)
 constexpr int kMaxGroups = 8;      // temporal groups per envelope family
-constexpr int kMaxStages = 7;
+constexpr int kMaxStages = 16;  // weights of one stage sum (NSRK78: 13)
 
 }  // namespace phx

@@ -89,36 +89,38 @@ __global__ void scatter_interior_kernel(const cx<T>* __restrict__ src, cx<T>* __
     }
 }
 
-// ---- DP45 error norm as the reference takes it over one halo-padded subgrid
-// (halo 7; adaptTimeStep sums rk_error and |buffer_wavefunction_plus|^2 over
-// every padded cell, solver.cu:73-75, cuda_matrix.cuh:614-632,699-705).
-// A padded point at ring distance rho (1..6) holds the stage value written
-// last there, Y_{8-rho} = y0 + stage sum m = 7-rho, and only k_1..k_m were
-// ever computed that far out, so its error term uses e_1..e_m.  Along
-// periodic axes those cells are exact copies of the wrapped interior point;
-// along zero axes they are the computed ring values, stored in place.
+// ---- Adaptive error norm as the reference takes it over one halo-padded
+// subgrid (halo H = k_max; adaptTimeStep sums rk_error and
+// |buffer_wavefunction_plus|^2 over every padded cell, solver.cu:73-75,
+// cuda_matrix.cuh:614-632,699-705).  Stage s computes k_s out to ring H - s
+// and intermediate sum m writes Y_{m+1} out to ring H - m, so a padded point
+// at ring distance rho (1..H-1) holds Y_{m+1} of sum m = min(S, H - rho) and
+// only k_1..k_{H-rho} were ever computed there: its error term uses those.
+// Along periodic axes those cells are exact copies of the wrapped interior
+// point; along zero axes they are the computed ring values, stored in place.
 template <typename T>
 struct RingParams {
     const cx<T>* psi0;  // state (y0)
     const cx<T>* k;     // k-stack, plane stride
     long long pitch, plane;
     int N_r, N_c, periodic_x, periodic_y;
+    int H, S, E;       // halo, solution-sum index, error weights
     T dt;
     T dtw1;            // dt * a21 (single-weight first stage sum)
-    T a[7][7];         // stage-sum weights, row m-1 builds Y_{m+1}
-    int nw[7];
-    T e[7];            // error weights
+    T a[kMaxStages][kMaxStages];  // stage-sum weights, row m-1 builds Y_{m+1} (row S-1: the solution)
+    int nw[kMaxStages];
+    T e[kMaxStages];   // error weights
     int passes;        // 1, or 2 where the reference counts the plus error twice
     double* partials;  // per-block (error, norm)
     // stochastic dw term of the stage sums (as in the stage kernels)
     NoiseParams noise;
-    T noise_amp, w_sum[7], R, gamma_c, four_dV, noise_scale;
+    T noise_amp, w_sum[kMaxStages], R, gamma_c, four_dV, noise_scale;
     const T* n0;       // state reservoir, or nullptr without reservoir
 };
 
 template <typename T>
 __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
-    const int B = 6;
+    const int B = R.H - 1;
     const long long W = R.N_c + 2LL * B;
     const long long band_tb = (long long)B * W, band_lr = (long long)R.N_r * B;
     const long long total = 2 * band_tb + 2 * band_lr;
@@ -140,9 +142,10 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
         const int sr = (dr && R.periodic_y) ? (r + R.N_r) % R.N_r : r;
         const int sc = (dc && R.periodic_x) ? (c + R.N_c) % R.N_c : c;
         const long long idx = (long long)sr * R.pitch + sc;
-        const int m = 7 - rho;
+        const int kv = R.H - rho;           // k_1..k_kv exist here
+        const int m = min(R.S, kv);         // buffer holds Y_{m+1}
         cx<T> e = mk((T)0, (T)0);
-        for (int j = 0; j < m; ++j) {
+        for (int j = 0; j < min(R.E, kv); ++j) {
             if (R.e[j] == (T)0) continue;
             e = cadd(e, smul(R.e[j], R.k[(long long)j * R.plane + idx]));
         }
@@ -152,8 +155,18 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
         if (m == 1) {
             y = cadd(y0, smul(R.dtw1, R.k[idx]));
         } else {
-            cx<T> acc = smul(R.a[m - 1][0], R.k[idx]);
-            for (int q = 1; q < R.nw[m - 1]; ++q) acc = cadd(acc, smul(R.a[m - 1][q], R.k[(long long)q * R.plane + idx]));
+            // as the stage kernels: up to 7 weights left to right, more nested from the right
+            const int n = R.nw[m - 1];
+            const bool wide = n > 7;
+            cx<T> acc = mk((T)0, (T)0);
+            bool have = false;
+            for (int u = 0; u < n; ++u) {
+                const int q = wide ? n - 1 - u : u;
+                if (wide && R.a[m - 1][q] == (T)0) continue;
+                const cx<T> tq = smul(R.a[m - 1][q], R.k[(long long)q * R.plane + idx]);
+                acc = !have ? tq : (wide ? cadd(tq, acc) : cadd(acc, tq));
+                have = true;
+            }
             y = cadd(y0, smul(R.dt, acc));
         }
         if (R.noise.on) {
@@ -185,14 +198,14 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
     }
 }
 
-// Outer ring (rho == 7) of the state's synchronised halo: images along
+// Outer ring (rho == H) of the state's synchronised halo: images along
 // periodic axes, zero outside any zero axis.  The reference's buffer keeps
 // this ring from the state of the previous accepted step (buffers swap on
 // accept, solver.cu:107-114), so the host carries the value one step.
 template <typename T>
 __global__ void ring7_kernel(const cx<T>* __restrict__ psi0, long long pitch, int N_r, int N_c, int periodic_x,
-                             int periodic_y, double* __restrict__ out) {
-    const int B = 7;
+                             int periodic_y, int H, double* __restrict__ out) {
+    const int B = H;
     const long long W = N_c + 2LL * B;
     const long long total = 2 * W + 2LL * (N_r + 2 * (B - 1));
     double a = 0.0;
@@ -223,7 +236,6 @@ __global__ void ring7_kernel(const cx<T>* __restrict__ psi0, long long pitch, in
     }
 }
 
-// Sum of n (error, norm) pairs in a fixed order: one block, deterministic.
 static __global__ void finalize_pairs_kernel(const double* __restrict__ partials, long long n, double* __restrict__ out) {
     __shared__ double sa[32], sb[32];
     double a = 0.0, b = 0.0;

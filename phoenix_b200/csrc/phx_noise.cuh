@@ -15,8 +15,9 @@
 //   r = sqrt(-2 ln u1); ln, cos and sin by the series below, in float, every
 //   operation rounded on its own so that results do not depend on the
 //   compiler's contraction choices.
-// The point id numbers padded coordinates (row + 8)(N_c + 16) + col + 8
-// after wrapping periodic axes: a periodic image draws its point's value.
+// The point id numbers padded coordinates (row + 16)(N_c + 32) + col + 16
+// after wrapping periodic axes (rings up to 15 deep): a periodic image draws
+// its point's value.
 #pragma once
 
 #include <cstdint>
@@ -103,7 +104,7 @@ __device__ __forceinline__ void noise_normal2(const NoiseParams& N, uint32_t poi
 __device__ __forceinline__ uint32_t noise_point(int r, int c, int N_r, int N_c, int periodic_x, int periodic_y) {
     if (periodic_y) r = r < 0 ? r + N_r : (r >= N_r ? r - N_r : r);
     if (periodic_x) c = c < 0 ? c + N_c : (c >= N_c ? c - N_c : c);
-    return (uint32_t)(r + 8) * (uint32_t)(N_c + 16) + (uint32_t)(c + 8);
+    return (uint32_t)(r + 16) * (uint32_t)(N_c + 32) + (uint32_t)(c + 16);
 }
 
 // xi = (z0, z1) * amp: the reference's random_number[i]

@@ -111,7 +111,7 @@ struct EngineBase {
 
 template <typename T>
 struct Engine final : EngineBase {
-    static constexpr int G = kRing;
+    int G = kRing;  // ring width of the padded planes: kRing, or H + 1 for wider halos
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
@@ -124,6 +124,7 @@ struct Engine final : EngineBase {
     Derived<T> d{};
     int comps = 1;
     int H = 4;  // halo width the reference uses: k_max of the iterator
+    Tableau tab;  // the fixed-step tableau of the other iterators
 
     // state and work planes (each allocation holds 1 or more planes)
     DevBuf psi[2], nres[2];            // state per component
@@ -168,7 +169,10 @@ struct Engine final : EngineBase {
         N_r = P.N_r;
         N_c = P.N_c;
         comps = P.tetm ? 2 : 1;
-        H = P.iterator == PHX_ITER_DP45 ? 7 : 4;
+        if (P.iterator != PHX_ITER_RK4 && !tableau_resolve(P.iterator, tab)) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
+        // halo_size_ = k_max_ of the iterator's constructor; the ring holds it
+        H = P.iterator == PHX_ITER_RK4 ? 4 : tab.H;
+        G = std::max(kRing, H + 1);
         pitch = ((N_c + 2LL * G) + 31) / 32 * 32;
         rows = N_r + 2LL * G;
         plane = pitch * rows;
@@ -187,8 +191,9 @@ struct Engine final : EngineBase {
                 acc_psi[q].alloc(cb, stream);
                 acc_n[q].alloc(rb, stream);
             } else {
-                k_psi[q].alloc(cb * 7, stream);
-                k_n[q].alloc(rb * 7, stream);
+                const int kp = std::max({7, tab.H, tab.nb, tab.E});
+                k_psi[q].alloc(cb * kp, stream);
+                k_n[q].alloc(rb * kp, stream);
             }
             pump[q].alloc(rb * std::max(1, P.n_pump_groups), stream);
             pot[q].alloc(rb * std::max(1, P.n_potential_groups), stream);
@@ -575,6 +580,15 @@ struct Engine final : EngineBase {
     void tensor_map(CUtensorMap* m, void* alloc_base, bool complex, int box_w_points, int box_h) {
         plane_tensor_map<T>(m, alloc_base, complex, pitch, rows, box_w_points, box_h);
     }
+    struct MapPair {
+        const void* psi = nullptr;
+        const void* n = nullptr;
+        CUtensorMap psi_map, n_map;
+    };
+    MapPair tma_maps[2];
+    int tma_next = 0;
+    CUtensorMap tma_pump_map, tma_pot_map;
+    bool tma_inputs_ready = false;
     template <bool RES, int TW, int TH, int NT>
     void go_tma(const FusedParams<T>& F) {
         using Lay = TmaLayout<T, TW, TH>;
@@ -590,13 +604,32 @@ struct Engine final : EngineBase {
         TmaParams<T> Q;
         std::memset(&Q, 0, sizeof(Q));
         Q.f = F;
-        // tensor maps over whole allocations (padded (0,0) = interior (-G,-G))
-        tensor_map(&Q.psi_map, reinterpret_cast<char*>(cplane(psi[0])) - sizeof(C) * (G * pitch + G), true, TW + 8, TH + 8);
-        tensor_map(&Q.n_map, reinterpret_cast<char*>(rplane(nres[0])) - sizeof(T) * (G * pitch + G), false, TW + 8, TH + 6);
+        // tensor maps over whole allocations (padded (0,0) = interior (-G,-G));
+        // the state alternates between two planes, so two encodings are kept
+        MapPair* mp = nullptr;
+        for (auto& m : tma_maps)
+            if (m.psi == psi[0].p && m.n == nres[0].p) mp = &m;
+        if (!mp) {
+            mp = &tma_maps[tma_next];
+            tma_next ^= 1;
+            tensor_map(&mp->psi_map, reinterpret_cast<char*>(cplane(psi[0])) - sizeof(C) * (G * pitch + G), true, TW + 8,
+                       TH + 8);
+            tensor_map(&mp->n_map, reinterpret_cast<char*>(rplane(nres[0])) - sizeof(T) * (G * pitch + G), false, TW + 8,
+                       TH + 6);
+            mp->psi = psi[0].p;
+            mp->n = nres[0].p;
+        }
+        if (!tma_inputs_ready) {
+            tensor_map(&tma_pump_map, pump[0].p, false, TW + 8, TH + 6);
+            tensor_map(&tma_pot_map, pot[0].p, false, TW + 8, TH + 6);
+            tma_inputs_ready = true;
+        }
+        Q.psi_map = mp->psi_map;
+        Q.n_map = mp->n_map;
+        Q.pump_map = tma_pump_map;
+        Q.pot_map = tma_pot_map;
         Q.has_pump = F.pump != nullptr;
         Q.has_pot = F.pot != nullptr;
-        tensor_map(&Q.pump_map, pump[0].p, false, TW + 8, TH + 6);
-        tensor_map(&Q.pot_map, pot[0].p, false, TW + 8, TH + 6);
         Q.tiles_x = (N_c + TW - 1) / TW;
         Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
         Q.err = static_cast<int*>(err_flag.p);
@@ -712,51 +745,65 @@ struct Engine final : EngineBase {
         }
     }
 
-    // ------------------------------------------------------------ DP45
-    // Butcher tableau of DormandPrince45 (dormand_prince.cu:18-35,37-95) in the
-    // operand order of its INTERMEDIATE_SUM_K / ERROR_K calls.
-    static void dp45_rows(T a[7][7], int nw[7], T c[7], T e[7]) {
-        std::memset(a, 0, sizeof(T) * 49);
-        a[0][0] = (T)(1.0 / 5.0);
-        nw[0] = 1;
-        a[1][0] = (T)(3.0 / 40.0), a[1][1] = (T)(9.0 / 40.0);
-        nw[1] = 2;
-        a[2][0] = (T)(44.0 / 45.0), a[2][1] = (T)(-56.0 / 15.0), a[2][2] = (T)(32.0 / 9.0);
-        nw[2] = 3;
-        a[3][0] = (T)(19372.0 / 6561.0), a[3][1] = (T)(-25360.0 / 2187.0), a[3][2] = (T)(64448.0 / 6561.0),
-        a[3][3] = (T)(-212.0 / 729.0);
-        nw[3] = 4;
-        a[4][0] = (T)(9017.0 / 3168.0), a[4][1] = (T)(-355.0 / 33.0), a[4][2] = (T)(46732.0 / 5247.0),
-        a[4][3] = (T)(49.0 / 176.0), a[4][4] = (T)(-5103.0 / 18656.0);
-        nw[4] = 5;
-        a[5][0] = (T)(35.0 / 384.0), a[5][1] = (T)(0.0), a[5][2] = (T)(500.0 / 1113.0), a[5][3] = (T)(125.0 / 192.0),
-        a[5][4] = (T)(-2187.0 / 6784.0), a[5][5] = (T)(11.0 / 84.0);
-        nw[5] = 6;
-        nw[6] = 7;
-        c[0] = (T)0.0, c[1] = (T)(1.0 / 5.0), c[2] = (T)(3.0 / 10.0), c[3] = (T)(4.0 / 5.0), c[4] = (T)(8.0 / 9.0),
-        c[5] = (T)1.0, c[6] = (T)1.0;
-        e[0] = (T)(35.0 / 384.0 - 5179.0 / 57600.0);
-        e[1] = (T)(0.0);
-        e[2] = (T)(500.0 / 1113.0 - 7571.0 / 16695.0);
-        e[3] = (T)(125.0 / 192.0 - 393.0 / 640.0);
-        e[4] = (T)(-2187.0 / 6784.0 + 92097.0 / 339200.0);
-        e[5] = (T)(11.0 / 84.0 - 187.0 / 2100.0);
-        e[6] = (T)(-1.0 / 40.0);
+    // ------------------------------------------------------------ other tableaux
+    // Stage s: k_s = f(Y_s) kept in the k-stack and Y_{s+1} = y0 + dt sum a_sq k_q
+    // over the subgrid extended by H - s; the last stage adds dt sum b_q k_q to
+    // the state in place (CALCULATE_K / INTERMEDIATE_SUM_K / FINAL_SUM_K).
+    void step_tableau() {
+        // a one-stage method (Newton) reads its stencil from the state, so its
+        // sum goes to a stage plane that then becomes the state
+        const bool single = tab.S == 1;
+        for (int s = 1; s <= tab.S; ++s) {
+            const bool last = s == tab.S;
+            StageParams<T> S = base_params(0);
+            set_coefficients(S, (T)tab.c[s - 1]);
+            region(S, last ? 0 : H - s);
+            S.stage = s;
+            S.nw = last ? tab.nb : tab.nw[s - 1];
+            for (int q = 0; q < S.nw; ++q) S.w[q] = (T)(last ? tab.b[q] : tab.a[s - 1][q]);
+            if (S.nw == 1) S.dtw = dt * S.w[0];
+            S.w_sum = right_fold(S.w, S.nw);
+            auto wire = [this, s, last, single](StageParams<T>& X, int q) {
+                X.psi0 = cplane(psi[q]);
+                X.n0 = rplane(nres[q]);
+                X.psi_in = s == 1 ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 2) & 1]);
+                X.n_in = s == 1 ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 2) & 1]);
+                X.k_psi = cplane(k_psi[q]);
+                X.k_n = rplane(k_n[q]);
+                X.psi_out = last && !single ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 1) & 1]);
+                X.n_out = last && !single ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 1) & 1]);
+                X.pump = rplane(pump[q]);
+                X.pot = rplane(pot[q]);
+                X.pulse = cplane(pulse[q]);
+            };
+            if (last)
+                launch<kStackFinal>(S, wire);
+            else
+                launch<kStack>(S, wire);
+        }
+        if (single) swap_state_with(0);
     }
 
-    long long dp45_stages(bool adaptive, bool ref_norm = false) {
-        T a[7][7], c[7], e[7];
-        int nw[7];
-        dp45_rows(a, nw, c, e);
-        for (int s = 1; s <= 6; ++s) {
+    // ------------------------------------------------------------ adaptive tableaux
+    // DP45, BoSha, CashKarp, Fehlberg2/5, DP85, NSRK78 (tableaux in
+    // phx_host.hpp): stages 1..S, then either the final sum in place (fixed
+    // dt) or the solution sum into a stage plane, an extra stage S + 1 for
+    // first-same-as-last tableaux, the error sum and the norm (FP64), and
+    // Solver::adaptTimeStep on the host.
+    T row_w(int m, int q) const { return (T)(m < tab.S - 1 ? tab.a[m][q] : tab.b[q]); }
+    int row_n(int m) const { return m < tab.S - 1 ? tab.nw[m] : tab.nb; }
+    int sol_slot() const { return (tab.S - 1) & 1; }
+    long long adaptive_stages(bool adaptive, bool ref_norm = false) {
+        const int S_ = tab.S;
+        for (int s = 1; s <= S_; ++s) {
             StageParams<T> S = base_params(0);
-            set_coefficients(S, c[s - 1]);
-            const bool final_fixed = !adaptive && s == 6;
-            region(S, final_fixed ? 0 : 7 - s);
+            set_coefficients(S, (T)tab.c[s - 1]);
+            const bool final_fixed = !adaptive && s == S_;
+            region(S, final_fixed ? 0 : H - s);
             S.stage = s;
-            S.nw = nw[s - 1];
-            for (int q = 0; q < S.nw; ++q) S.w[q] = a[s - 1][q];
-            if (S.nw == 1) S.dtw = dt * a[s - 1][0];
+            S.nw = row_n(s - 1);
+            for (int q = 0; q < S.nw; ++q) S.w[q] = row_w(s - 1, q);
+            if (S.nw == 1) S.dtw = dt * S.w[0];
             S.w_sum = right_fold(S.w, S.nw);
             auto wire = [this, s, final_fixed](StageParams<T>& X, int q) {
                 X.psi0 = cplane(psi[q]);
@@ -777,20 +824,22 @@ struct Engine final : EngineBase {
                 launch<kStack>(S, wire);
         }
         if (!adaptive) return 0;
-        // k7 = f(y6) and the error / norm reduction over the interior
+        // error (e_1..e_E; k_{S+1} = f(solution) for first-same-as-last tableaux,
+        // evaluated but unused otherwise) and the solution's norm over the interior
         StageParams<T> S = base_params(0);
-        set_coefficients(S, c[6]);
+        set_coefficients(S, (T)tab.c[tab.fsal ? S_ : S_ - 1]);
         region(S, 0);
-        S.stage = 7;
-        S.nw = 7;
-        for (int q = 0; q < 7; ++q) S.w[q] = e[q];
+        S.stage = S_ + 1;
+        S.nw = tab.E;
+        for (int q = 0; q < tab.E; ++q) S.w[q] = (T)tab.e[q];
         S.partials = reinterpret_cast<double*>(partials.p);
         S.error_passes = P.tetm ? 2 : 1;
-        launch<kStackError>(S, [this](StageParams<T>& X, int q) {
+        const int slot = sol_slot();
+        launch<kStackError>(S, [this, slot](StageParams<T>& X, int q) {
             X.psi0 = cplane(psi[q]);
             X.n0 = rplane(nres[q]);
-            X.psi_in = cplane(sbuf_psi[q][1]);
-            X.n_in = rplane(sbuf_n[q][1]);
+            X.psi_in = cplane(sbuf_psi[q][slot]);
+            X.n_in = rplane(sbuf_n[q][slot]);
             X.k_psi = cplane(k_psi[q]);
             X.k_n = rplane(k_n[q]);
             X.pump = rplane(pump[q]);
@@ -809,18 +858,23 @@ struct Engine final : EngineBase {
             R.N_c = N_c;
             R.periodic_x = P.periodic_x;
             R.periodic_y = P.periodic_y;
+            R.H = H;
+            R.S = S_;
             R.dt = dt;
-            R.dtw1 = dt * a[0][0];
-            std::memcpy(R.a, a, sizeof(R.a));
-            std::memcpy(R.nw, nw, sizeof(R.nw));
-            std::memcpy(R.e, e, sizeof(R.e));
+            R.dtw1 = dt * row_w(0, 0);
+            for (int m = 0; m < S_; ++m) {
+                R.nw[m] = row_n(m);
+                for (int q = 0; q < R.nw[m]; ++q) R.a[m][q] = row_w(m, q);
+            }
+            R.E = tab.E;
+            for (int q = 0; q < tab.E; ++q) R.e[q] = (T)tab.e[q];
             R.passes = P.tetm ? 2 : 1;
             R.partials = reinterpret_cast<double*>(partials.p) + 2 * nb;
             {
                 const StageParams<T> B = base_params(0);
                 R.noise = B.noise;
                 R.noise_amp = B.noise_amp;
-                for (int m = 0; m < 7; ++m) R.w_sum[m] = nw[m] ? right_fold(a[m], nw[m]) : (T)0;
+                for (int m = 0; m < S_; ++m) R.w_sum[m] = right_fold(R.a[m], R.nw[m]);
                 R.R = B.R;
                 R.gamma_c = B.gamma_c;
                 R.four_dV = B.four_dV;
@@ -836,14 +890,14 @@ struct Engine final : EngineBase {
     }
 
     bool adapt_time_step(double err_sum, double norm_sum) {
-        // Solver::adaptTimeStep with power 1/4 (solver.cu:72-105)
+        // Solver::adaptTimeStep (solver.cu:72-105) with the tableau's power
         const T normalization_factor = (T)norm_sum;
         const T integrated_error = (T)err_sum;
         T final_error = std::abs(integrated_error / normalization_factor);
         const T tol = (T)P.tol;
         const T lo = std::numeric_limits<T>::min();
         const T dh_arg = (T)((double)tol / 2.0 / (double)(final_error > lo ? final_error : lo));
-        T dh = (T)std::pow((double)dh_arg, (double)(T)0.25);
+        T dh = std::pow(dh_arg, (T)tab.power);  // std::pow<Type::real>(dh_arg, Type::real(power))
         if (std::isnan(dh)) {
             dh = (T)0.9;
             final_error = std::numeric_limits<T>::max();
@@ -860,10 +914,12 @@ struct Engine final : EngineBase {
         return final_error < tol;
     }
 
-    void swap_state_with_y6() {
+    // the stage plane `slot` becomes the state (and the state a stage plane);
+    // rings along zero axes are zeroed again
+    void swap_state_with(int slot) {
         for (int q = 0; q < comps; ++q) {
-            std::swap(psi[q].p, sbuf_psi[q][1].p);
-            std::swap(nres[q].p, sbuf_n[q][1].p);
+            std::swap(psi[q].p, sbuf_psi[q][slot].p);
+            std::swap(nres[q].p, sbuf_n[q][slot].p);
             if (!(P.periodic_x && P.periodic_y)) {
                 ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(psi[q]), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
                 ring_fill_kernel<T><<<64, 256, 0, stream>>>(rplane(nres[q]), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
@@ -873,22 +929,24 @@ struct Engine final : EngineBase {
         }
     }
 
-    void step_dp45(bool adaptive, int64_t& acc, int64_t& rej) {
+    void step_adaptive(bool adaptive, int64_t& acc, int64_t& rej) {
+        if (tab.inverted) return step_inverted(adaptive, acc, rej);
         if (!adaptive) {
-            dp45_stages(false);
+            adaptive_stages(false);
             return;
         }
         const bool ref_norm = P.norm_mode == PHX_NORM_REFERENCE;
         if (ref_norm) {
-            // outer ring of the state's halo at the start of this step -> result[2]
-            ring7_kernel<T><<<1, 1024, 0, stream>>>(cplane(psi[0]), pitch, N_r, N_c, P.periodic_x, P.periodic_y,
+            // outer ring H of the state's halo at the start of this step -> result[2]
+            ring7_kernel<T><<<1, 1024, 0, stream>>>(cplane(psi[0]), pitch, N_r, N_c, P.periodic_x, P.periodic_y, H,
                                                     reinterpret_cast<double*>(result.p) + 2);
             ++launches;
             PHX_CUDA(cudaGetLastError());
         }
         bool accept = false;
+        int rejections = 0;
         do {
-            const long long nb = dp45_stages(true, ref_norm);
+            const long long nb = adaptive_stages(true, ref_norm);
             finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), nb,
                                                           reinterpret_cast<double*>(result.p));
             ++launches;
@@ -905,13 +963,81 @@ struct Engine final : EngineBase {
             }
             accept = adapt_time_step(err, nrm);
             if (accept) {
-                swap_state_with_y6();
+                swap_state_with(sol_slot());
                 r7_prev = r7_cur;
                 ++acc;
             } else {
                 ++rej;
+                if (++rejections > kMaxRejections)
+                    fail(PHX_ERR_NONFINITE, "step size control rejected " + std::to_string(kMaxRejections) +
+                                                " attempts in a row (non-finite error norm?)");
             }
         } while (!accept);
+    }
+    static constexpr int kMaxRejections = 100000;
+
+    // DormandPrince85::step as the reference has it (dormand_prince.cu:182-190):
+    // its fixed and variable branches are swapped.  Fixed dt: the solution goes
+    // to the buffer and is dropped, the state stays as it is.  Variable dt: the
+    // final sum is added to the state in place and no error is formed (the
+    // error array keeps its zeros), so adaptTimeStep accepts with dt -> dt_max
+    // unless the buffer's norm is zero or not finite, and the swap makes the
+    // buffer -- the stage-12 input -- the state.
+    void step_inverted(bool adaptive, int64_t& acc, int64_t& rej) {
+        if (!adaptive) return;
+        int rejections = 0;
+        for (;;) {
+            // stages 1 .. S-1 leave Y_S in a stage plane (k_S and the in-place sum
+            // end up in the plane the swap hands back to the buffer)
+            const int S_ = tab.S;
+            for (int s = 1; s < S_; ++s) {
+                StageParams<T> S = base_params(0);
+                set_coefficients(S, (T)tab.c[s - 1]);
+                region(S, H - s);
+                S.stage = s;
+                S.nw = row_n(s - 1);
+                for (int q = 0; q < S.nw; ++q) S.w[q] = row_w(s - 1, q);
+                if (S.nw == 1) S.dtw = dt * S.w[0];
+                S.w_sum = right_fold(S.w, S.nw);
+                launch<kStack>(S, [this, s](StageParams<T>& X, int q) {
+                    X.psi0 = cplane(psi[q]);
+                    X.n0 = rplane(nres[q]);
+                    X.psi_in = s == 1 ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 2) & 1]);
+                    X.n_in = s == 1 ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 2) & 1]);
+                    X.k_psi = cplane(k_psi[q]);
+                    X.k_n = rplane(k_n[q]);
+                    X.psi_out = cplane(sbuf_psi[q][(s - 1) & 1]);
+                    X.n_out = rplane(sbuf_n[q][(s - 1) & 1]);
+                    X.pump = rplane(pump[q]);
+                    X.pot = rplane(pot[q]);
+                    X.pulse = cplane(pulse[q]);
+                });
+            }
+            const int slot = (S_ - 2) & 1;
+            // normalization_factor = sum |buffer|^2; integrated_error = 0
+            FieldRef f{&sbuf_psi[0][slot], true, 0, 0};
+            const double nrm = plane_norm(f);
+            const bool ok = adapt_time_step(0.0, nrm);
+            if (ok) {
+                swap_state_with(slot);
+                ++acc;
+                return;
+            }
+            ++rej;
+            if (++rejections > kMaxRejections) fail(PHX_ERR_NONFINITE, "DP85 buffer norm is zero or not finite");
+        }
+    }
+    double plane_norm(const FieldRef& f) {
+        const int blocks = 296;
+        sum_abs2_kernel<T, true><<<blocks, 256, 0, stream>>>(reinterpret_cast<const T*>(cplane(*f.buf)), pitch, N_r, N_c,
+                                                             reinterpret_cast<double*>(partials.p));
+        finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), blocks,
+                                                      reinterpret_cast<double*>(result.p));
+        launches += 2;
+        PHX_CUDA(cudaGetLastError());
+        PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        PHX_CUDA(cudaStreamSynchronize(stream));
+        return static_cast<const double*>(host_result.p)[0];
     }
 
     // ------------------------------------------------------------ FFT filter
@@ -947,7 +1073,6 @@ struct Engine final : EngineBase {
         const int64_t l0 = launches;
         int64_t its = 0, acc = 0, rej = 0, filt = 0;
         const T t_max = (T)P.t_max, fft_every = (T)P.fft_every;
-        const bool dp45 = P.iterator == PHX_ITER_DP45;
         while (its < max_iterations) {
             if (t >= t_max) break;
             if (P.stochastic_amplitude > 0.0) noise_amp = (T)P.stochastic_amplitude * std::sqrt(dt);
@@ -958,10 +1083,12 @@ struct Engine final : EngineBase {
                 ta = get_event();
                 PHX_CUDA(cudaEventRecord(ta, stream));
             }
-            if (dp45) {
-                step_dp45(P.adaptive != 0, acc, rej);
-            } else {
+            if (P.iterator == PHX_ITER_RK4) {
                 step_rk4();
+            } else if (tab.adaptive) {
+                step_adaptive(P.adaptive != 0, acc, rej);
+            } else {
+                step_tableau();
             }
             if (shape < 0) tune_record(ta, tb);
             ++its;
@@ -1312,8 +1439,13 @@ void validate(const phx_params& p) {
     if ((long long)p.N_c * p.N_r > (1LL << 31)) fail(PHX_ERR_INVALID_ARG, "grid too large");
     if (p.dtype != PHX_F32 && p.dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "dtype must be PHX_F32 or PHX_F64");
     if (p.dtype == PHX_F32 && (p.N_c & 1)) fail(PHX_ERR_UNSUPPORTED, "FP32 grids need an even N_c");
-    if (p.iterator != PHX_ITER_RK4 && p.iterator != PHX_ITER_DP45) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
-    if (p.adaptive && p.iterator != PHX_ITER_DP45) fail(PHX_ERR_INVALID_ARG, "adaptive stepping needs DP45");
+    if (p.iterator < PHX_ITER_RK4 || p.iterator > PHX_ITER_NSRK78) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
+    {
+        phx::Tableau t;
+        if (p.adaptive && (p.iterator == PHX_ITER_RK4 || !phx::tableau_resolve(p.iterator, t) || !t.adaptive))
+            fail(PHX_ERR_INVALID_ARG, "adaptive stepping needs an adaptive iterator (DP45, BoSha, CashKarp, Fehlberg2, "
+                                      "Fehlberg5, DP85, NSRK78)");
+    }
     if (p.norm_mode != PHX_NORM_REFERENCE && p.norm_mode != PHX_NORM_INTERIOR) fail(PHX_ERR_INVALID_ARG, "bad norm_mode");
     if (!(p.L_x > 0) || !(p.L_y > 0) || !(p.h_bar_s > 0) || !(p.m_eff > 0)) fail(PHX_ERR_INVALID_ARG, "L, h_bar_s and m_eff must be > 0");
     if (!(p.dt > 0)) fail(PHX_ERR_INVALID_ARG, "dt must be > 0");

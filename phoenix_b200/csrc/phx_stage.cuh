@@ -362,9 +362,16 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
                                 out_wf.v[j] = cadd(y0.v[j], smul(P.dtw, out_wf.v[j]));
                                 if constexpr (RES) out_rv.v[j] = radd(n0.v[j], rmul(P.dtw, out_rv.v[j]));
                             } else {
-                                cx<T> a;
+                                // up to 7 weights: left to right, zeros included
+                                // (runge_sum_to_input_k2..k7); more: zeros dropped, nested
+                                // from the right (sum_single_k, kernel_summation.cuh:7-29)
+                                const bool wide = P.nw > 7;
+                                cx<T> a = mk((T)0, (T)0);
                                 T an = (T)0;
-                                for (int q = 0; q < P.nw; ++q) {
+                                bool have = false;
+                                for (int u = 0; u < P.nw; ++u) {
+                                    const int q = wide ? P.nw - 1 - u : u;
+                                    if (wide && P.w[q] == (T)0) continue;
                                     cx<T> kq;
                                     T kqn = (T)0;
                                     if (q == P.stage - 1) {
@@ -374,12 +381,14 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
                                         kq = ld1(P.k_psi + (long long)q * P.plane + idx + j);
                                         if constexpr (RES) kqn = P.k_n[(long long)q * P.plane + idx + j];
                                     }
-                                    if (q == 0) {
-                                        a = smul(P.w[0], kq);
-                                        an = rmul(P.w[0], kqn);
+                                    const cx<T> tq = smul(P.w[q], kq);
+                                    const T tn = rmul(P.w[q], kqn);
+                                    if (!have) {
+                                        a = tq, an = tn, have = true;
+                                    } else if (wide) {
+                                        a = cadd(tq, a), an = radd(tn, an);
                                     } else {
-                                        a = cadd(a, smul(P.w[q], kq));
-                                        an = radd(an, rmul(P.w[q], kqn));
+                                        a = cadd(a, tq), an = radd(an, tn);
                                     }
                                 }
                                 out_wf.v[j] = cadd(y0.v[j], smul(P.dt, a));

@@ -272,9 +272,15 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                                 orp.v[j] = radd(n0p.v[j], rmul(P.dtw, orp.v[j]));
                                 orm.v[j] = radd(n0m.v[j], rmul(P.dtw, orm.v[j]));
                             } else {
-                                cx<T> a1, a2;
+                                // summation order as in the scalar kernel (7 weights or fewer:
+                                // left to right; more: zeros dropped, nested from the right)
+                                const bool wide = P.nw > 7;
+                                cx<T> a1 = mk((T)0, (T)0), a2 = mk((T)0, (T)0);
                                 T b1 = (T)0, b2 = (T)0;
-                                for (int q = 0; q < P.nw; ++q) {
+                                bool have = false;
+                                for (int u = 0; u < P.nw; ++u) {
+                                    const int q = wide ? P.nw - 1 - u : u;
+                                    if (wide && P.w[q] == (T)0) continue;
                                     cx<T> k1, k2;
                                     T kn1, kn2;
                                     if (q == P.stage - 1) {
@@ -283,12 +289,14 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                                         const long long o = (long long)q * P.plane + idx + j;
                                         k1 = ld1(P.k_psi + o), k2 = ld1(Q.k_psi + o), kn1 = P.k_n[o], kn2 = Q.k_n[o];
                                     }
-                                    if (q == 0) {
-                                        a1 = smul(P.w[0], k1), a2 = smul(P.w[0], k2);
-                                        b1 = rmul(P.w[0], kn1), b2 = rmul(P.w[0], kn2);
+                                    const cx<T> t1 = smul(P.w[q], k1), t2 = smul(P.w[q], k2);
+                                    const T u1 = rmul(P.w[q], kn1), u2 = rmul(P.w[q], kn2);
+                                    if (!have) {
+                                        a1 = t1, a2 = t2, b1 = u1, b2 = u2, have = true;
+                                    } else if (wide) {
+                                        a1 = cadd(t1, a1), a2 = cadd(t2, a2), b1 = radd(u1, b1), b2 = radd(u2, b2);
                                     } else {
-                                        a1 = cadd(a1, smul(P.w[q], k1)), a2 = cadd(a2, smul(P.w[q], k2));
-                                        b1 = radd(b1, rmul(P.w[q], kn1)), b2 = radd(b2, rmul(P.w[q], kn2));
+                                        a1 = cadd(a1, t1), a2 = cadd(a2, t2), b1 = radd(b1, u1), b2 = radd(b2, u2);
                                     }
                                 }
                                 owp.v[j] = cadd(y0p.v[j], smul(P.dt, a1));

@@ -309,10 +309,29 @@ class Solver:
 
 
 class SolverFactory:
-    """REGISTER_SOLVER keys of the hot path (runge_kutta.cu:96, dormand_prince.cu:97)."""
+    """REGISTER_SOLVER keys of the reference (source/cuda_solver/solver/iterator/*.cu), matched
+    case-insensitively like the CLI's --iterator."""
     registry: Dict[str, Tuple[bool, str]] = {
         "RK4": (False, "Runge-Kutta 4"),
         "DP45": (True, "Dormand-Prince 5(4) method for time integration."),
+        "RK3": (False, "Runge-Kutta 3"),
+        "SSPRK3": (False, "Strong Stability Preserving Runge Kutta 3"),
+        "MP": (False, "MidPoint"),
+        "HEUN2": (False, "Heun2"),
+        "HEUN3": (False, "Heun3"),
+        "HW": (False, "Houwen-Wray"),
+        "NEWTON": (False, "Newton"),
+        "NYSTROEM": (False, "Nystroem's fifth-order method"),
+        "RALSTON": (False, "Ralston 2nd order method for time integration."),
+        "RALSTON3": (False, "Ralston 3rd order method for time integration."),
+        "RALSTON4": (False, "Ralston 4th order method for time integration."),
+        "RULE38": (False, "Third-order Runge-Kutta method (3/8 rule)"),
+        "BOSHA": (True, "Bogacki-Shampine 3(2)"),
+        "CASHKARP": (True, "Cash-Karp 5(4)"),
+        "FEHLBERG2": (True, "Fehlberg 2(1) order method for time integration."),
+        "FEHLBERG5": (True, "Fehlberg 5(4) order method for time integration."),
+        "DP85": (True, "Dormand–Prince 8(5) method for time integration."),
+        "NSRK78": (True, "Nullspace RK 13-stage 8th order"),
     }
 
     @classmethod

@@ -198,6 +198,38 @@ def cases():
     c["tetm_f64_zero"] = dict(grid, **STRONG, dtype="f64", iterator="RK4", tetm=1, dt=0.01,
                               t_max=0.2 * (1 - 1e-9), periodic_x=0, periodic_y=0, seed=21, psi_amp=1.0,
                               pumps=[(4.0, 3.0, 0.0)])
+    # the fixed-step tableaux of the reference's other registered iterators:
+    # mixed boundaries (periodic x, zero y) so the extended stage regions of
+    # the zero axis are exercised, pump + potential, 20 steps
+    # (RK3 and Ralston4 are left out: the reference's RK3 final sum lists a
+    # fourth weight and reads a k plane past its three-plane stack, and its
+    # Ralston4 declares k_max 3 for four stages and writes past the stack;
+    # neither output is defined)
+    for k, (it, seed) in enumerate([("SSPRK3", 32), ("MP", 33), ("Heun2", 34), ("Heun3", 35),
+                                    ("HW", 36), ("Newton", 37), ("Nystroem", 38), ("Ralston", 39),
+                                    ("Ralston3", 40), ("Rule38", 42)]):
+        c[f"tab_{it.lower()}_f64_mixed"] = dict(N_c=40, N_r=32, L_x=25.0, L_y=20.0, **STRONG, dtype="f64",
+                                                 iterator=it, dt=0.005, t_max=20 * 0.005 * (1 - 1e-9),
+                                                 periodic_x=1, periodic_y=0, seed=seed, psi_amp=1.0,
+                                                 n0_amp=0.5, pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
+    # adaptive tableaux (DP45 has its own cases above)
+    ad = dict(**STRONG, dtype="f64", adaptive=1, tol=1e-6, dt_min=1e-5, dt_max=0.05, dt=0.01, t_max=0.2,
+              psi_amp=1.0, pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
+    for it, (px, py), seed in [("BoSha", (1, 1), 51), ("CashKarp", (1, 0), 52), ("Fehlberg2", (0, 0), 53),
+                               ("Fehlberg5", (1, 1), 54), ("DP85", (1, 0), 55), ("NSRK78", (0, 0), 56)]:
+        c[f"tab_{it.lower()}_f64_adaptive"] = dict(grid, **ad, iterator=it, periodic_x=px, periodic_y=py, seed=seed)
+    c["tab_dp85_f64_fixed"] = dict(grid, **STRONG, dtype="f64", iterator="DP85", dt=0.01, t_max=10 * 0.01 * (1 - 1e-9),
+                                   periodic_x=0, periodic_y=0, seed=57, psi_amp=1.0, n0_amp=0.5,
+                                   pumps=[(4.0, 3.0, 0.0)])
+    c["tab_nsrk78_f64_fixed"] = dict(grid, **STRONG, dtype="f64", iterator="NSRK78", dt=0.01,
+                                     t_max=10 * 0.01 * (1 - 1e-9), periodic_x=1, periodic_y=0, seed=58, psi_amp=1.0,
+                                     pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
+    c["tab_bosha_f32_fixed"] = dict(grid, **STRONG, dtype="f32", iterator="BoSha", dt=0.005,
+                                    t_max=20 * 0.005 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=59, psi_amp=1.0,
+                                    pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
+    c["tab_ssprk3_f32_periodic"] = dict(grid, **STRONG, dtype="f32", iterator="SSPRK3", dt=0.005,
+                                        t_max=20 * 0.005 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=43,
+                                        psi_amp=1.0, pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
     return c
 
 
