@@ -27,6 +27,8 @@ Legs of the JSON line:
              after another through single-simulation handles
   adjoint    the inverse-design gradient: 512^2 FP32, 500 RK4 iterations, device
              time of the plain forward, the checkpointed forward and the backward
+  configs    the other configurations: 256^2 FP64 RK4, 1024^2 FP64 RK4 and DP45
+             adaptive (FP32, FP64), FP32-vs-FP64 error, 4096^2 TE/TM FP32 with noise
 `--impl reference` runs that reference CPU build alone (rank 0 of any launch).
 """
 from __future__ import annotations
@@ -380,13 +382,108 @@ def run_adjoint(pb, torch, device, iters=500, n=512):
             e2.record(st)
         torch.cuda.synchronize()
         times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+    # per-kernel device time of one more forward + backward (library events)
+    s.profile(True)
+    P.grad = None
+    psi_T, _ = evolve(s, P, z0, m0, iters)
+    (((psi_T.real ** 2 + psi_T.imag ** 2) - rho_t) ** 2).sum().backward()
+    torch.cuda.synchronize()
+    kernels = {k: {"ms": v["ms"], "launches": v["launches"]} for k, v in s.profile_read().items()}
     s.close()
     fwd, bwd = times[-1]
     return {"grid": [n, n], "iterations": iters, "dtype": "f32", "checkpoint_every": int(np.ceil(np.sqrt(iters))),
+            "kernels_forward_and_backward": kernels,
             "plain_forward_ms": plain_ms, "checkpointed_forward_ms": fwd, "backward_ms": bwd,
             "backward_over_plain_forward": bwd / plain_ms,
-            "note": "backward = recompute of every segment with the stage kernels + 4 vector-Jacobian launches per "
-                    "iteration; loss evaluation by torch between the two"}
+            "note": "backward = per iteration one fused recompute launch (stage values stored) + one fused "
+                    "vector-Jacobian launch; loss evaluation by torch between the two"}
+
+
+def _device_us(torch, solver, device, iters):
+    """Device time per iteration of `iters` iterations (CUDA events on the solver stream)."""
+    st = torch.cuda.ExternalStream(solver.stream, device=device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(st):
+        a.record(st)
+    info = solver.run(iters)
+    with torch.cuda.stream(st):
+        b.record(st)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) * 1e3 / max(info.iterations, 1), info
+
+
+def run_configs(pb, torch, device):
+    """The other configurations: 256^2 FP64 RK4 (1000 steps); 1024^2 FP64 RK4,
+    DP45 adaptive (rtol 1e-6) in FP32 and FP64 and the FP32-vs-FP64 error of
+    RK4; 4096^2 TE/TM FP32 RK4 with a ring pump and noise (dw 1e-3) and its
+    deterministic twin.  Device time per iteration after the launch-shape
+    autotuning (40 untimed iterations)."""
+    out = {}
+    dev = device
+
+    def sysp(n, dtype, it="RK4", **kw):
+        dt = kw.pop("dt", dt_for(n))
+        return pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                                   periodic_boundary_y=True, dtype=dtype, iterator=it, dt=dt, t0=0.0, t_max=1e12,
+                                   fft_every=1e12, pump_temporal=[pb.Temporal()], device=dev, **kw)
+
+    # config 1: 256^2 FP64 RK4, dt 0.04, 1000 steps
+    n = 256
+    wl = workload(n, seed=1)
+    with pb.Solver(sysp(n, "f64", dt=0.04)) as s:
+        s.set_field("psi_plus", wl["psi0"])
+        s.set_field("pump_plus", wl["pump"], 0)
+        s.run(40)
+        us, info = _device_us(torch, s, dev, 1000)
+        out["rk4_256_f64"] = {"us_per_iteration": us, "iterations": info.iterations, "launch_shape": info.launch_shape}
+    # config 2: 1024^2 -- FP64 RK4, FP32 vs FP64, DP45 adaptive
+    n = 1024
+    wl = workload(n)
+    finals = {}
+    for dtype in ("f32", "f64"):
+        with pb.Solver(sysp(n, dtype, potential_temporal=[pb.Temporal()])) as s:
+            s.set_field("psi_plus", wl["psi0"])
+            s.set_field("pump_plus", wl["pump"], 0)
+            s.set_field("potential_plus", wl["potential"], 0)
+            s.run(40)
+            us, info = _device_us(torch, s, dev, 460)
+            finals[dtype] = s.get_field("psi_plus").astype(np.complex128)
+            out[f"rk4_1024_{dtype}"] = {"us_per_iteration": us, "launch_shape": info.launch_shape}
+    out["fp32_vs_fp64_rel_l2_after_500_rk4"] = float(np.linalg.norm(finals["f32"] - finals["f64"]) /
+                                                     np.linalg.norm(finals["f64"]))
+    for dtype in ("f32", "f64"):
+        sp = sysp(n, dtype, it="DP45", potential_temporal=[pb.Temporal()], use_adaptive_timestep=True,
+                  tolerance=1e-6, dt_min=1e-5, dt_max=0.05)
+        with pb.Solver(sp) as s:
+            s.set_field("psi_plus", wl["psi0"])
+            s.set_field("pump_plus", wl["pump"], 0)
+            s.set_field("potential_plus", wl["potential"], 0)
+            s.run(20)
+            us, info = _device_us(torch, s, dev, 100)
+            out[f"dp45_adaptive_1024_{dtype}"] = {"us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
+                                                  "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt}
+    # config 3: 4096^2 TE/TM FP32, ring pump r 20 um w 3 um, delta_LT 0.05, g_pm = -0.2 g_c, dt 0.0015
+    n = 4096
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n, dtype=np.float64)
+    X, Y = np.meshgrid(x, x)
+    ring = (1.5 * P_TH * np.exp(-(np.sqrt(X ** 2 + Y ** 2) - 20.0) ** 2 / (2 * 3.0 ** 2))).astype(np.float32)
+    del X, Y
+    rng = np.random.default_rng(4)
+    for dw in (1e-3, 0.0):
+        sp = sysp(n, "f32", dt=0.0015, use_twin_mode=True, stochastic_amplitude=dw, random_seed=4)
+        sp.g_pm, sp.delta_LT = -0.2 * PHYS["g_c"], 0.05
+        with pb.Solver(sp) as s:
+            for comp in ("plus", "minus"):
+                psi0 = (1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
+                s.set_field(f"psi_{comp}", psi0)
+                s.set_field(f"pump_{comp}", ring, 0)
+            s.run(12)
+            us, info = _device_us(torch, s, dev, 20)
+            key = "tetm_4096_f32_noise" if dw else "tetm_4096_f32_deterministic"
+            out[key] = {"us_per_iteration": us, "grid_point_updates_per_s": 2 * n * n / (us * 1e-6),
+                        "launch_shape": info.launch_shape}
+    return out
 
 
 def config_dict(args):
@@ -412,6 +509,8 @@ def main():
     ap.add_argument("--sweep-instances", type=int, default=256, help="instances of the batched sweep (0: skip)")
     ap.add_argument("--sweep-steps", type=int, default=200, help="timed iterations of the batched sweep")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (inverse-design) leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' timings")
+    ap.add_argument("--only", choices=["configs", "adjoint", "sweep"], help="run one leg alone and print its JSON")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -421,6 +520,16 @@ def main():
 
     import phoenix_b200 as pb
 
+    if args.only:
+        import torch
+
+        import phoenix_b200 as pb
+
+        torch.cuda.set_device(0)
+        leg = {"configs": lambda: run_configs(pb, torch, 0), "adjoint": lambda: run_adjoint(pb, torch, 0),
+               "sweep": lambda: run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, 0)}[args.only]
+        print(json.dumps({args.only: leg()}))
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -596,6 +705,9 @@ def main():
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         adjoint = run_adjoint(pb, torch, local)
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = run_configs(pb, torch, local)
 
     if rank == 0:
         us = step_ms * 1e3
@@ -613,7 +725,7 @@ def main():
                              "step_frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},
                 "kernel_avg_ms": kernels_ms, "launch_shape": shape, "gpu_launches": launches, "fft_filters_in_timed_region": filters,
                 "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu, "sweep": sweep,
-                "adjoint": adjoint}
+                "adjoint": adjoint, "configs": configs}
         print(json.dumps(line))
     if dist:
         dist.barrier()

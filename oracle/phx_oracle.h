@@ -17,6 +17,8 @@
  *                             nystroem.cu:30-56, ralston.cu:31-41,66-80,106-124, rule38.cu:28-47
  *   the adaptive tableaux     bogacki.cu:27-76, cash_karp.cu:31-84, fehlberg.cu:33-73,100-153,
  *                             dormand_prince.cu:128-204, NSRK78.cu:37-117
+ *   SSFM::step                split_step_fourier_method.cu:24-72 with the SSFM kernels
+ *                             (kernel_gp_compute.cuh:244-440)
  *   gp_scalar                 include/kernel/kernel_gp_compute.cuh:18-236
  *   runge_sum_to_input_k / runge_add_to_input_k / runge_sum_to_error
  *                             include/kernel/kernel_summation.cuh:66-289
@@ -48,7 +50,7 @@ enum {
     PHX_ORACLE_HEUN2 = 5, PHX_ORACLE_HEUN3 = 6, PHX_ORACLE_HW = 7, PHX_ORACLE_NEWTON = 8, PHX_ORACLE_NYSTROEM = 9,
     PHX_ORACLE_RALSTON = 10, PHX_ORACLE_RALSTON3 = 11, PHX_ORACLE_RALSTON4 = 12, PHX_ORACLE_RULE38 = 13,
     PHX_ORACLE_BOSHA = 14, PHX_ORACLE_CASHKARP = 15, PHX_ORACLE_FEHLBERG2 = 16, PHX_ORACLE_FEHLBERG5 = 17,
-    PHX_ORACLE_DP85 = 18, PHX_ORACLE_NSRK78 = 19
+    PHX_ORACLE_DP85 = 18, PHX_ORACLE_NSRK78 = 19, PHX_ORACLE_SSFM = 20
 };
 enum { PHX_ORACLE_T_CONSTANT = 0, PHX_ORACLE_T_IEXP = 1, PHX_ORACLE_T_COS = 2, PHX_ORACLE_T_GAUSS = 3 };
 

@@ -23,7 +23,7 @@ TEMPORAL = {"constant": 0, "iexp": 1, "osc": 1, "cos": 2, "gauss": 3}
 # REGISTER_SOLVER keys of the reference, numbered as in include/phx.h
 ITERATORS = {"RK4": 0, "DP45": 1, "RK3": 2, "SSPRK3": 3, "MP": 4, "HEUN2": 5, "HEUN3": 6, "HW": 7, "NEWTON": 8,
              "NYSTROEM": 9, "RALSTON": 10, "RALSTON3": 11, "RALSTON4": 12, "RULE38": 13, "BOSHA": 14,
-             "CASHKARP": 15, "FEHLBERG2": 16, "FEHLBERG5": 17, "DP85": 18, "NSRK78": 19}
+             "CASHKARP": 15, "FEHLBERG2": 16, "FEHLBERG5": 17, "DP85": 18, "NSRK78": 19, "SSFM": 20}
 
 
 class Temporal(C.Structure):

@@ -171,3 +171,176 @@ __global__ void unpack_interior_kernel(const V* __restrict__ dense, V* __restric
 }
 
 }  // namespace phx
+
+namespace phx {
+
+// The four vector-Jacobian stages of one iteration in one launch.  A block
+// owns a TW x TH tile; lam' is staged in shared memory with a 4-cell halo,
+// Ybar_s (psi part, needed with a stencil by stage s - 1) ping-pongs between
+// two shared buffers, stage s evaluated on the tile plus a (s - 1)-cell halo
+// (4: 3 cells, ..., 1: none).  The n parts are pointwise and stay in
+// registers, as do the running sum of Ybar and the pump gradient.  The new
+// lam is written with 4-deep periodic images (the next iteration reads it
+// with a 4-cell halo).  Same arithmetic as adj_stage_kernel, periodic
+// boundaries only.
+template <typename T>
+struct AdjFusedParams {
+    int N_r, N_c;
+    long long pitch;
+    const cx<T>* Ypsi[4];  // Y_1 .. Y_4
+    const T* Yn[4];
+    const cx<T>* lam_psi;  // lam' (4-deep images)
+    const T* lam_n;
+    cx<T>* out_psi;        // lam (another plane)
+    T* out_n;
+    const T* pot;
+    T* pbar;
+    T c_pot[4], c_pump[4];
+    T dt_b[4], a_dt[4];    // dt b_s; a_s dt (a_4 unused)
+    T A, ohb, ohb_gc, ohb_gr, half_R, half_gamma_c, gamma_r, R;
+    T m2, odx2, ody2;
+    int res;
+};
+
+template <typename V>
+__device__ __forceinline__ void adj_images4(int N_r, int N_c, long long pitch, V* base, int r, int c, V v) {
+    const bool lx = c < 4, hx = c >= N_c - 4, ly = r < 4, hy = r >= N_r - 4;
+    if (!(lx || hx || ly || hy)) return;
+    const int cs = lx ? c + N_c : c - N_c;
+    const int rs = ly ? r + N_r : r - N_r;
+    if (lx || hx) base[(long long)r * pitch + cs] = v;
+    if (ly || hy) base[(long long)rs * pitch + c] = v;
+    if ((lx || hx) && (ly || hy)) base[(long long)rs * pitch + cs] = v;
+}
+
+template <typename T, int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) adj_fused_kernel(const __grid_constant__ AdjFusedParams<T> Q) {
+    constexpr int W4 = TW + 8, H4 = TH + 8;  // lam' with a 4-cell halo
+    constexpr int W3 = TW + 6, H3 = TH + 6;  // Ybar regions (3-cell halo at most)
+    constexpr int NP = W3 * H3;
+    constexpr int OWN = (NP + NT - 1) / NT;
+    __shared__ cx<T> sL[H4 * W4];
+    __shared__ cx<T> sB[2][H3 * W3];
+    const int ty0 = blockIdx.y * TH, tx0 = blockIdx.x * TW;
+    const long long p = Q.pitch;
+    // every load stays within rows / columns [-4, N + 4) of the padded planes
+    // (ring >= 8); cells beyond feed no output point of this tile
+    for (int k = threadIdx.x; k < H4 * W4; k += NT) {
+        const int y = k / W4, x = k - y * W4;
+        const int r = ty0 - 4 + y, c = tx0 - 4 + x;
+        sL[k] = (r < Q.N_r + 4 && c < Q.N_c + 4) ? Q.lam_psi[(long long)r * p + c] : mk((T)0, (T)0);
+    }
+    __syncthreads();
+    T ybn[OWN], accn[OWN], pb[OWN];
+    cx<T> acc[OWN];
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        ybn[j] = (T)0, accn[j] = (T)0, pb[j] = (T)0;
+        acc[j] = mk((T)0, (T)0);
+    }
+#pragma unroll
+    for (int s = 4; s >= 1; --s) {
+        const int h = s - 1;  // halo of this stage's region
+        const cx<T>* prev = sB[(s + 1) & 1];
+        cx<T>* cur = sB[s & 1];
+        const T dtb = Q.dt_b[s - 1], adt = s < 4 ? Q.a_dt[s - 1] : (T)0;
+        auto mu_at = [&](int qy, int qx) {  // kbar_s psi at W3-grid point (qy, qx) (may be a halo-4 point)
+            cx<T> m = sL[(qy + 1) * W4 + qx + 1];
+            m.re *= dtb;
+            m.im *= dtb;
+            if (s < 4) {
+                const cx<T> y = prev[qy * W3 + qx];
+                m.re += adt * y.re;
+                m.im += adt * y.im;
+            }
+            return m;
+        };
+#pragma unroll
+        for (int j = 0; j < OWN; ++j) {
+            const int q = threadIdx.x + NT * j;
+            if (q >= NP) continue;
+            const int qy = q / W3, qx = q - qy * W3;  // W3 grid: tile offset -3
+            const int dy = qy - 3, dx = qx - 3;      // offset from the tile origin
+            if (dy < -h || dy >= TH + h || dx < -h || dx >= TW + h) continue;
+            const int r = ty0 + dy, c = tx0 + dx;
+            if (r >= Q.N_r + 4 || c >= Q.N_c + 4) {
+                cur[qy * W3 + qx] = mk((T)0, (T)0);
+                ybn[j] = (T)0;
+                continue;
+            }
+            const long long i = (long long)r * p + c;
+            const cx<T> mu = mu_at(qy, qx);
+            // neighbours: stage 4 reads lam' only (halo 4 in sL); lower stages read Ybar_{s+1}
+            // on its region, one cell wider than this one
+            cx<T> mu_u, mu_d, mu_l, mu_r;
+            if (s == 4) {
+                auto lam_mu = [&](int yy, int xx) {
+                    cx<T> m = sL[(yy + 1) * W4 + xx + 1];
+                    m.re *= dtb;
+                    m.im *= dtb;
+                    return m;
+                };
+                mu_u = lam_mu(qy - 1, qx), mu_d = lam_mu(qy + 1, qx), mu_l = lam_mu(qy, qx - 1), mu_r = lam_mu(qy, qx + 1);
+            } else {
+                mu_u = mu_at(qy - 1, qx), mu_d = mu_at(qy + 1, qx), mu_l = mu_at(qy, qx - 1), mu_r = mu_at(qy, qx + 1);
+            }
+            T m = (T)0;
+            if (Q.res) m = dtb * Q.lam_n[i] + adt * ybn[j];
+            const cx<T> psi = Q.Ypsi[s - 1][i];
+            const T n = Q.res ? Q.Yn[s - 1][i] : (T)0;
+            const T norm = psi.re * psi.re + psi.im * psi.im;
+            cx<T> lap;
+            lap.re = Q.m2 * mu.re + Q.ody2 * (mu_u.re + mu_d.re) + Q.odx2 * (mu_l.re + mu_r.re);
+            lap.im = Q.m2 * mu.im + Q.ody2 * (mu_u.im + mu_d.im) + Q.odx2 * (mu_l.im + mu_r.im);
+            T W = Q.ohb_gc * norm;
+            T B = -Q.half_gamma_c;
+            if (Q.res) {
+                W += Q.ohb_gr * n;
+                B += Q.half_R * n;
+            }
+            if (Q.pot) W += Q.ohb * (Q.pot[i] * Q.c_pot[s - 1]);
+            const T hre = Q.A * lap.re + W * mu.re, him = Q.A * lap.im + W * mu.im;
+            const T im_mbar_psi = mu.re * psi.im - mu.im * psi.re;
+            const T re_mbar_psi = mu.re * psi.re + mu.im * psi.im;
+            const T sp = (T)2 * Q.ohb_gc * im_mbar_psi - (Q.res ? (T)2 * Q.R * n * m : (T)0);
+            cx<T> g;
+            g.re = -him + B * mu.re + sp * psi.re;
+            g.im = hre + B * mu.im + sp * psi.im;
+            T gn = (T)0;
+            if (Q.res) gn = Q.ohb_gr * im_mbar_psi + Q.half_R * re_mbar_psi - (Q.gamma_r + Q.R * norm) * m;
+            cur[qy * W3 + qx] = g;
+            ybn[j] = gn;
+            if (dy >= 0 && dy < TH && dx >= 0 && dx < TW) {
+                acc[j].re += g.re;
+                acc[j].im += g.im;
+                accn[j] += gn;
+                pb[j] += Q.c_pump[s - 1] * m;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        const int q = threadIdx.x + NT * j;
+        if (q >= NP) continue;
+        const int qy = q / W3, qx = q - qy * W3;
+        const int dy = qy - 3, dx = qx - 3;
+        if (dy < 0 || dy >= TH || dx < 0 || dx >= TW) continue;
+        const int r = ty0 + dy, c = tx0 + dx;
+        if (r >= Q.N_r || c >= Q.N_c) continue;
+        const long long i = (long long)r * p + c;
+        cx<T> l = sL[(qy + 1) * W4 + qx + 1];
+        l.re += acc[j].re;
+        l.im += acc[j].im;
+        Q.out_psi[i] = l;
+        adj_images4(Q.N_r, Q.N_c, p, Q.out_psi, r, c, l);
+        if (Q.res) {
+            const T ln = Q.lam_n[i] + accn[j];
+            Q.out_n[i] = ln;
+            adj_images4(Q.N_r, Q.N_c, p, Q.out_n, r, c, ln);
+            if (Q.pbar) Q.pbar[i] += pb[j];
+        }
+    }
+}
+
+}  // namespace phx

@@ -68,6 +68,20 @@ __global__ void mask_kernel(cx<T>* __restrict__ data, const T* __restrict__ mask
     }
 }
 
+// the same, on the interior of a halo-padded plane (in-place transform)
+template <typename T>
+__global__ void mask_padded_kernel(cx<T>* __restrict__ base, long long pitch, int N_r, int N_c, const T* __restrict__ mask) {
+    const long long n = (long long)N_r * N_c;
+    const T fn = (T)n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / N_c, c = i - r * N_c;
+        cx<T>* p = base + r * pitch + c;
+        const cx<T> d = *p;
+        const T m = mask[i];
+        *p = mk(rmul(rdiv(d.re, fn), m), rmul(rdiv(d.im, fn), m));
+    }
+}
+
 // contiguous -> padded interior, plus periodic images
 template <typename T>
 __global__ void scatter_interior_kernel(const cx<T>* __restrict__ src, cx<T>* __restrict__ dst, long long pitch, int N_r,

@@ -371,11 +371,24 @@ struct Engine final : EngineBase {
         if (pp) *pp = pitch;
     }
 
+    // The reference plans (N_c, N_r) on the full N_r x N_c matrix
+    // (solver_fft.cu:35-48).  Square grids transform the halo-padded state
+    // plane in place (advanced layout: rows of `pitch` elements), with no
+    // copies in or out; other shapes reinterpret the row-major matrix as N_c
+    // rows of N_r, which only a contiguous copy can express.
+    bool fft_in_place = false;
     void ensure_fft() {
         if (have_plan) return;
-        fft_x.alloc(sizeof(C) * (size_t)N_r * N_c, stream);
-        // the reference plans (N_c, N_r) on the full N_r x N_c matrix (solver_fft.cu:35-48)
-        PHX_CUFFT(cufftPlan2d(&plan, N_c, N_r, sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z));
+        fft_in_place = N_r == N_c && !std::getenv("PHX_FFT_CONTIGUOUS");
+        if (fft_in_place) {
+            int n[2] = {N_r, N_c};
+            int embed[2] = {(int)rows, (int)pitch};
+            PHX_CUFFT(cufftPlanMany(&plan, 2, n, embed, 1, (int)plane, embed, 1, (int)plane,
+                                    sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z, 1));
+        } else {
+            fft_x.alloc(sizeof(C) * (size_t)N_r * N_c, stream);
+            PHX_CUFFT(cufftPlan2d(&plan, N_c, N_r, sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z));
+        }
         PHX_CUFFT(cufftSetStream(plan, stream));
         have_plan = true;
     }
@@ -1048,6 +1061,19 @@ struct Engine final : EngineBase {
             const int blocks = (int)std::min<long long>((N + 255) / 256, 148 * 16);
             cudaEvent_t a = nullptr;
             prof_begin(a);
+            if (fft_in_place) {
+                // applyFFTFilter on the padded plane itself: FFT, (data / N) * mask,
+                // inverse FFT, then the ring's images / zeros again
+                C* base = cplane(psi[q]);
+                exec_fft_on(base, CUFFT_FORWARD);
+                mask_padded_kernel<T><<<blocks, 256, 0, stream>>>(base, pitch, N_r, N_c, reinterpret_cast<const T*>(mask[q].p));
+                exec_fft_on(base, CUFFT_INVERSE);
+                ring_fill_kernel<C><<<64, 256, 0, stream>>>(base, N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
+                prof_end(PHX_KERNEL_FILTER, a, (double)N * (4 * sizeof(C) + sizeof(T)));
+                launches += 2;
+                PHX_CUDA(cudaGetLastError());
+                continue;
+            }
             gather_interior_kernel<T><<<blocks, 256, 0, stream>>>(cplane(psi[q]), pitch, N_r, N_c, reinterpret_cast<C*>(fft_x.p));
             exec_fft(CUFFT_FORWARD);
             mask_kernel<T><<<blocks, 256, 0, stream>>>(reinterpret_cast<C*>(fft_x.p), reinterpret_cast<const T*>(mask[q].p), N);
@@ -1057,6 +1083,14 @@ struct Engine final : EngineBase {
             prof_end(PHX_KERNEL_FILTER, a, (double)N * (6 * sizeof(C) + sizeof(T)));
             launches += 3;
             PHX_CUDA(cudaGetLastError());
+        }
+    }
+    void exec_fft_on(C* data, int dir) {
+        if constexpr (sizeof(T) == 4) {
+            PHX_CUFFT(cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(data), reinterpret_cast<cufftComplex*>(data), dir));
+        } else {
+            PHX_CUFFT(cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(data), reinterpret_cast<cufftDoubleComplex*>(data),
+                                   dir));
         }
     }
     void exec_fft(int dir) {
@@ -1186,6 +1220,9 @@ struct Engine final : EngineBase {
     int64_t adj_T = 0, adj_every = 0;
     T adj_dt = 0;
     bool adj_ready = false;
+    // one fused launch per iteration (adj_fused_kernel); PHX_ADJOINT_STAGES=1
+    // selects the four-launch path (adj_stage_kernel)
+    bool adj_fused = !(std::getenv("PHX_ADJOINT_STAGES") && std::atoi(std::getenv("PHX_ADJOINT_STAGES")) == 1);
 
     void adjoint_check() {
         if (P.iterator != PHX_ITER_RK4 || P.tetm) fail(PHX_ERR_UNSUPPORTED, "the adjoint covers scalar fixed-step RK4");
@@ -1265,6 +1302,40 @@ struct Engine final : EngineBase {
                 launch<kRk4Last>(S, wire);
         }
     }
+    // the same in one launch: the fused iteration kernel that also stores the
+    // stage values (bit-identical to the stage kernels)
+    void rk4_recompute_fused(DevBuf& yp, DevBuf* yn, DevBuf* sp[3], DevBuf* sn[3], DevBuf& op, DevBuf* on) {
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        FusedParams<T> F;
+        std::memset(&F, 0, sizeof(F));
+        for (int s = 0; s < 4; ++s) {
+            if (P.n_pump_groups) F.pump_c[s] = interp<T>(amp_pump[0], next_pump[0], cw[s]).real();
+            if (P.n_potential_groups) F.pot_c[s] = interp<T>(amp_pot[0], next_pot[0], cw[s]).real();
+        }
+        fused_constants<T>(F, P, d, dt, pitch);
+        F.psi0 = cplane(yp);
+        F.n0 = yn ? rplane(*yn) : nullptr;
+        F.psi1 = cplane(op);
+        F.n1 = on ? rplane(*on) : nullptr;
+        F.pump = P.n_pump_groups ? rplane(pump[0]) : nullptr;
+        F.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
+        for (int s = 0; s < 3; ++s) {
+            F.st_psi[s] = cplane(*sp[s]);
+            F.st_n[s] = sn[s] ? rplane(*sn[s]) : nullptr;
+        }
+        constexpr int TW = 32, TH = sizeof(T) == 4 ? 32 : 16;
+        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        if (P.use_reservoir)
+            rk4_fused_kernel<T, true, TW, TH, 256, true><<<grid, 256, 0, stream>>>(F);
+        else
+            rk4_fused_kernel<T, false, TW, TH, 256, true><<<grid, 256, 0, stream>>>(F);
+        const double st = sizeof(C) + (P.use_reservoir ? sizeof(T) : 0);
+        prof_end(PHX_KERNEL_RK4_FUSED, a, (double)N_r * N_c * (5 * st + (P.n_pump_groups ? sizeof(T) : 0)));
+        ++launches;
+        PHX_CUDA(cudaGetLastError());
+    }
     void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump) override {
         if (!adj_ready) fail(PHX_ERR_STATE, "phx_adjoint_forward must run first");
         if (!dpsi) fail(PHX_ERR_INVALID_ARG, "dL/dpsi_T is NULL");
@@ -1318,9 +1389,59 @@ struct Engine final : EngineBase {
                                  res ? st_n[3 * j + 2].get() : nullptr};
                 DevBuf& op = j + 1 < len ? *sg_psi[j + 1] : scratch_psi;
                 DevBuf* on = res ? (j + 1 < len ? sg_n[j + 1].get() : &scratch_n) : nullptr;
-                rk4_recompute(*sg_psi[j], res ? sg_n[j].get() : nullptr, sp, sn, op, on);
+                if (adj_fused)
+                    rk4_recompute_fused(*sg_psi[j], res ? sg_n[j].get() : nullptr, sp, sn, op, on);
+                else
+                    rk4_recompute(*sg_psi[j], res ? sg_n[j].get() : nullptr, sp, sn, op, on);
             }
             for (int64_t j = len - 1; j >= 0; --j) {
+                if (adj_fused) {
+                    AdjFusedParams<T> Q;
+                    std::memset(&Q, 0, sizeof(Q));
+                    Q.N_r = N_r;
+                    Q.N_c = N_c;
+                    Q.pitch = pitch;
+                    Q.Ypsi[0] = cplane(*sg_psi[j]);
+                    Q.Yn[0] = res ? rplane(*sg_n[j]) : nullptr;
+                    for (int s = 2; s <= 4; ++s) {
+                        Q.Ypsi[s - 1] = cplane(*st_psi[3 * j + s - 2]);
+                        Q.Yn[s - 1] = res ? rplane(*st_n[3 * j + s - 2]) : nullptr;
+                    }
+                    Q.lam_psi = cplane(lam_psi[cur]);
+                    Q.lam_n = res ? rplane(lam_n[cur]) : nullptr;
+                    Q.out_psi = cplane(lam_psi[cur ^ 1]);
+                    Q.out_n = res ? rplane(lam_n[cur ^ 1]) : nullptr;
+                    Q.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
+                    Q.pbar = (res && P.n_pump_groups) ? rplane(pbar) : nullptr;
+                    for (int s = 1; s <= 4; ++s) {
+                        Q.c_pot[s - 1] = P.n_potential_groups ? interp<T>(amp_pot[0], next_pot[0], cw[s - 1]).real() : (T)0;
+                        Q.c_pump[s - 1] = P.n_pump_groups ? interp<T>(amp_pump[0], next_pump[0], cw[s - 1]).real() : (T)0;
+                        Q.dt_b[s - 1] = adj_dt * bw[s - 1];
+                        Q.a_dt[s - 1] = s < 4 ? aw[s - 1] * adj_dt : (T)0;
+                    }
+                    Q.A = d.ohb * d.meff;
+                    Q.ohb = d.ohb;
+                    Q.ohb_gc = d.ohb * (T)P.g_c;
+                    Q.ohb_gr = d.ohb * (T)P.g_r;
+                    Q.half_R = (T)0.5 * (T)P.R;
+                    Q.half_gamma_c = (T)0.5 * (T)P.gamma_c;
+                    Q.gamma_r = (T)P.gamma_r;
+                    Q.R = (T)P.R;
+                    Q.m2 = d.m2;
+                    Q.odx2 = d.odx2;
+                    Q.ody2 = d.ody2;
+                    Q.res = res;
+                    constexpr int TW = 32, TH = 16;
+                    dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+                    cudaEvent_t a = nullptr;
+                    prof_begin(a);
+                    adj_fused_kernel<T, TW, TH, 256><<<grid, 256, 0, stream>>>(Q);
+                    prof_end(PHX_KERNEL_OTHER, a, (double)N_r * N_c * (5.0 * sizeof(C) + 7.0 * sizeof(T)));
+                    ++launches;
+                    PHX_CUDA(cudaGetLastError());
+                    cur ^= 1;
+                    continue;
+                }
                 for (int s = 4; s >= 1; --s) {
                     AdjParams<T> Q;
                     std::memset(&Q, 0, sizeof(Q));

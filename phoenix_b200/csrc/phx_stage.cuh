@@ -193,11 +193,18 @@ __device__ __forceinline__ void rhs_scalar(const StageParams<T>& P, long long id
 // gamma_c) / (4 dV)) with n0 the state reservoir (kernel_summation.cuh:216-224);
 // the reference's product with the complex square root (x, 0) keeps each
 // component's two roundings
+template <typename T>
+__device__ __forceinline__ cx<T> stage_xi(const StageParams<T>& P, int r, int c) {
+    return noise_xi(P.noise, noise_point(r, c, P.N_r, P.N_c, P.img_x, P.img_y), P.noise_amp);
+}
 template <typename T, bool RES>
-__device__ __forceinline__ cx<T> stage_noise(const StageParams<T>& P, int r, int c, T n0) {
-    const cx<T> xi = noise_xi(P.noise, noise_point(r, c, P.N_r, P.N_c, P.img_x, P.img_y), P.noise_amp);
+__device__ __forceinline__ cx<T> stage_noise_of(const StageParams<T>& P, cx<T> xi, T n0) {
     const T sc = RES ? rsqrt_rn(rdiv(radd(rmul(P.R, n0), P.gamma_c), P.four_dV)) : P.noise_scale;
     return mk(rmul(rmul(P.w_sum, xi.re), sc), rmul(rmul(P.w_sum, xi.im), sc));
+}
+template <typename T, bool RES>
+__device__ __forceinline__ cx<T> stage_noise(const StageParams<T>& P, int r, int c, T n0) {
+    return stage_noise_of<T, RES>(P, stage_xi(P, r, c), n0);
 }
 
 // Periodic images of a produced point (wavefunction and reservoir): every

@@ -227,9 +227,9 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                             // reservoir; the final sum updates n+ in place before the minus
                             // wavefunction's sum runs (cuda_macro.cuh:200-229), so psi- sees
                             // the new n+ there
-                            owp.v[j] = cadd(owp.v[j], stage_noise<T, true>(P, r, c + j, n0p.v[j]));
-                            owm.v[j] = cadd(owm.v[j],
-                                            stage_noise<T, true>(P, r, c + j, KIND == kRk4Last ? orp.v[j] : n0p.v[j]));
+                            const cx<T> xi = stage_xi(P, r, c + j);
+                            owp.v[j] = cadd(owp.v[j], stage_noise_of<T, true>(P, xi, n0p.v[j]));
+                            owm.v[j] = cadd(owm.v[j], stage_noise_of<T, true>(P, xi, KIND == kRk4Last ? orp.v[j] : n0p.v[j]));
                         }
                     }
                     if constexpr (KIND != kRk4Last) {
@@ -305,9 +305,10 @@ __global__ void __launch_bounds__(32 * WARPS) stage_tetm_kernel(const __grid_con
                                 orm.v[j] = radd(n0m.v[j], rmul(P.dt, b2));
                             }
                             if (P.noise.on) {
-                                owp.v[j] = cadd(owp.v[j], stage_noise<T, true>(P, r, c + j, n0p.v[j]));
-                                owm.v[j] = cadd(owm.v[j], stage_noise<T, true>(P, r, c + j,
-                                                                               KIND == kStackFinal ? orp.v[j] : n0p.v[j]));
+                                const cx<T> xi = stage_xi(P, r, c + j);
+                                owp.v[j] = cadd(owp.v[j], stage_noise_of<T, true>(P, xi, n0p.v[j]));
+                                owm.v[j] = cadd(owm.v[j],
+                                                stage_noise_of<T, true>(P, xi, KIND == kStackFinal ? orp.v[j] : n0p.v[j]));
                             }
                         }
                     }

@@ -48,6 +48,8 @@ struct FusedParams {
     T b[4];
     T dtw[3];
     T dt;
+    cx<T>* st_psi[3];  // STORE: the stage values Y2..Y4 (with images), for the adjoint
+    T* st_n[3];
 };
 
 constexpr int kImg = kImgDepth;
@@ -97,7 +99,7 @@ __device__ __forceinline__ void fused_images(const FusedParams<T>& P, V* base, i
 // registers; the stencil input of each stage is in shared memory.  Shared
 // planes are stored with one leading pad column so that every pair starts on
 // a 16-byte boundary.
-template <typename T, bool RES, int TW, int TH, int NT>
+template <typename T, bool RES, int TW, int TH, int NT, bool STORE = false>
 __global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ FusedParams<T> P) {
     static_assert(TW % 2 == 0, "pairs");
     constexpr int W4 = TW + 8, H4 = TH + 8;    // tile + 4-cell halo (stage-1 stencil input)
@@ -186,8 +188,21 @@ __global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ F
                     an[j][h] = radd(an[j][h], rmul(P.b[s], kr[h]));
                 }
                 if (s < 3) {
-                    out[e + h] = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
+                    const cx<T> o = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
+                    out[e + h] = o;
                     if constexpr (RES) ns[j][h] = radd(n0[j][h], rmul(P.dtw[s], kr[h]));
+                    if constexpr (STORE) {
+                        const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
+                        if (qy >= 3 && qy < H3 - 3 && qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {
+                            const long long g = (long long)gy * pitch + gx;
+                            P.st_psi[s][g] = o;
+                            if (P.img_x | P.img_y) fused_images(P, P.st_psi[s], gy, gx, o);
+                            if constexpr (RES) {
+                                P.st_n[s][g] = ns[j][h];
+                                if (P.img_x | P.img_y) fused_images(P, P.st_n[s], gy, gx, ns[j][h]);
+                            }
+                        }
+                    }
                 } else {
                     const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
                     if (qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {

@@ -227,6 +227,8 @@ def cases():
     c["tab_bosha_f32_fixed"] = dict(grid, **STRONG, dtype="f32", iterator="BoSha", dt=0.005,
                                     t_max=20 * 0.005 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=59, psi_amp=1.0,
                                     pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
+    # (no SSFM case: the reference CPU build ends its first SSFM step with a
+    # segmentation fault, with or without a k-space mask)
     c["tab_ssprk3_f32_periodic"] = dict(grid, **STRONG, dtype="f32", iterator="SSPRK3", dt=0.005,
                                         t_max=20 * 0.005 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=43,
                                         psi_amp=1.0, pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])

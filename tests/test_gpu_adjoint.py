@@ -159,3 +159,21 @@ def test_inverse_design_512_fp32_gradient_vs_fp64_central_differences(require_gp
         errs.append(abs(float(np.sum(gP.astype(np.float64) * v)) - fd) / abs(fd))
     print("inverse design 512^2: FP32 adjoint vs FP64 central differences, rel. errors", errs)
     assert max(errs) < 1e-2, errs
+
+
+def test_fused_adjoint_kernel_matches_stage_kernels(require_gpu, monkeypatch):
+    """The one-launch adjoint iteration and the four stage launches compute the
+    same vector-Jacobian products (summed in a different order): FP64 to 1e-12,
+    on a grid that is not a multiple of the tile."""
+    n, L, iters = 72, 100.0, 30
+    pump, rho, psi0 = inverse_design_inputs(n, L)
+    rng = np.random.default_rng(9)
+    psi0 = psi0 + 0.5 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    n0 = rng.random((n, n))
+    pot = 0.1 * rng.standard_normal((n, n))
+    sp = system(n, L, "f64", 0.04)
+    fused = adjoint_grads(sp, pump, psi0, n0, pot, rho, iters)
+    monkeypatch.setenv("PHX_ADJOINT_STAGES", "1")
+    staged = adjoint_grads(sp, pump, psi0, n0, pot, rho, iters)
+    for a, b in zip(fused[1:], staged[1:]):
+        assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b)

@@ -193,3 +193,16 @@ def test_bad_field_shape_is_rejected(require_gpu):
             s.set_field("psi_plus", np.zeros((16, 16)))
         with pytest.raises(pb.PhxError):
             s.get_field("pump_plus", 0)  # no pump groups configured
+
+
+def test_fft_filter_in_place_matches_contiguous_path(require_gpu, monkeypatch):
+    """Square grids filter the padded state plane in place (advanced cuFFT
+    layout); the contiguous gather/FFT/scatter path gives the same field to
+    rounding (FP64, 1e-13)."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "rk4_f64_mask.npz"))
+    case = json.loads(str(z["params"]))
+    fields = O.fields_from_golden(z)
+    a, _, _ = run_gpu(case, fields)
+    monkeypatch.setenv("PHX_FFT_CONTIGUOUS", "1")
+    b, _, _ = run_gpu(case, fields)
+    assert rel_l2(a["psi_plus"], b["psi_plus"]) <= 1e-13
