@@ -74,7 +74,8 @@ typedef enum {
     PHX_ITER_FEHLBERG2 = 16,/* "Fehlberg2" fehlberg.cu:75 (adaptive) */
     PHX_ITER_FEHLBERG5 = 17,/* "Fehlberg5" fehlberg.cu:155 (adaptive) */
     PHX_ITER_DP85 = 18,     /* "DP85"      dormand_prince.cu:206 (adaptive) */
-    PHX_ITER_NSRK78 = 19    /* "NSRK78"    NSRK78.cu:119 (adaptive) */
+    PHX_ITER_NSRK78 = 19,   /* "NSRK78"    NSRK78.cu:119 (adaptive) */
+    PHX_ITER_SSFM = 20      /* "SSFM"      split_step_fourier_method.cu:74 (split-step Fourier, periodic) */
 } phx_iterator;
 
 /* DP45 error norm.  PHX_NORM_REFERENCE reproduces the reference's sums over

@@ -20,7 +20,7 @@ STATUS = {0: "PHX_OK", 1: "PHX_ERR_INVALID_ARG", 2: "PHX_ERR_OOM", 3: "PHX_ERR_C
 F32, F64 = 0, 1
 ITER = {"RK4": 0, "DP45": 1, "RK3": 2, "SSPRK3": 3, "MP": 4, "HEUN2": 5, "HEUN3": 6, "HW": 7, "NEWTON": 8,
         "NYSTROEM": 9, "RALSTON": 10, "RALSTON3": 11, "RALSTON4": 12, "RULE38": 13, "BOSHA": 14, "CASHKARP": 15,
-        "FEHLBERG2": 16, "FEHLBERG5": 17, "DP85": 18, "NSRK78": 19}
+        "FEHLBERG2": 16, "FEHLBERG5": 17, "DP85": 18, "NSRK78": 19, "SSFM": 20}
 NORM_REFERENCE, NORM_INTERIOR = 0, 1
 FIELDS = {"psi_plus": 0, "psi_minus": 1, "n_plus": 2, "n_minus": 3, "pump_plus": 4, "pump_minus": 5,
           "potential_plus": 6, "potential_minus": 7, "pulse_plus": 8, "pulse_minus": 9, "fft_mask_plus": 10,

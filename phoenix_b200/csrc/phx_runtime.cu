@@ -31,6 +31,7 @@
 #include "phx_step_tma.cuh"
 #include "phx_rt.hpp"
 #include "phx_adjoint.cuh"
+#include "phx_ssfm.cuh"
 
 namespace phx {
 
@@ -159,6 +160,7 @@ struct Engine final : EngineBase {
         }
         for (auto e : event_pool) cudaEventDestroy(e);
         if (have_plan) cufftDestroy(plan);
+        if (have_ssfm_plan) cufftDestroy(ssfm_plan);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -169,9 +171,10 @@ struct Engine final : EngineBase {
         N_r = P.N_r;
         N_c = P.N_c;
         comps = P.tetm ? 2 : 1;
-        if (P.iterator != PHX_ITER_RK4 && !tableau_resolve(P.iterator, tab)) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
-        // halo_size_ = k_max_ of the iterator's constructor; the ring holds it
-        H = P.iterator == PHX_ITER_RK4 ? 4 : tab.H;
+        if (P.iterator != PHX_ITER_RK4 && P.iterator != PHX_ITER_SSFM && !tableau_resolve(P.iterator, tab))
+            fail(PHX_ERR_INVALID_ARG, "unknown iterator");
+        // halo_size_ = k_max_ of the iterator's constructor (SSFM: 0); the ring holds it
+        H = P.iterator == PHX_ITER_RK4 ? 4 : (P.iterator == PHX_ITER_SSFM ? 0 : tab.H);
         G = std::max(kRing, H + 1);
         pitch = ((N_c + 2LL * G) + 31) / 32 * 32;
         rows = N_r + 2LL * G;
@@ -1053,6 +1056,80 @@ struct Engine final : EngineBase {
         return static_cast<const double*>(host_result.p)[0];
     }
 
+    // ------------------------------------------------------------ SSFM
+    // SSFM::step (split_step_fourier_method.cu:24-72): four unnormalised
+    // transforms per iteration on contiguous copies of psi, with the
+    // reference's (N_c, N_r) plan; kernels in phx_ssfm.cuh.
+    DevBuf ssfm_w[2], ssfm_f[2];
+    cufftHandle ssfm_plan = 0;
+    bool have_ssfm_plan = false;
+    void ssfm_fft(C* in, C* out, int dir) {
+        if constexpr (sizeof(T) == 4) {
+            PHX_CUFFT(cufftExecC2C(ssfm_plan, reinterpret_cast<cufftComplex*>(in), reinterpret_cast<cufftComplex*>(out), dir));
+        } else {
+            PHX_CUFFT(cufftExecZ2Z(ssfm_plan, reinterpret_cast<cufftDoubleComplex*>(in), reinterpret_cast<cufftDoubleComplex*>(out),
+                                   dir));
+        }
+    }
+    void step_ssfm() {
+        const long long N = (long long)N_r * N_c;
+        if (!have_ssfm_plan) {
+            for (int q = 0; q < comps; ++q) {
+                ssfm_w[q].alloc(sizeof(C) * N, stream);
+                ssfm_f[q].alloc(sizeof(C) * N, stream);
+            }
+            PHX_CUFFT(cufftPlan2d(&ssfm_plan, N_c, N_r, sizeof(T) == 4 ? CUFFT_C2C : CUFFT_Z2Z));
+            PHX_CUFFT(cufftSetStream(ssfm_plan, stream));
+            have_ssfm_plan = true;
+        }
+        SsfmParams<T> S;
+        std::memset(&S, 0, sizeof(S));
+        S.N_r = N_r, S.N_c = N_c, S.pitch = pitch, S.tetm = P.tetm, S.res = P.use_reservoir;
+        S.hbs = (T)P.h_bar_s, S.meff = (T)P.m_eff, S.Lx = (T)P.L_x, S.Ly = (T)P.L_y, S.dt = dt, S.N2 = (T)(unsigned)N;
+        S.g_c = (T)P.g_c, S.g_r = (T)P.g_r, S.R = (T)P.R, S.gamma_c = (T)P.gamma_c, S.gamma_r = (T)P.gamma_r;
+        S.g_pm = (T)P.g_pm, S.ohb = d.ohb, S.dV = d.dV;
+        S.n_pump = P.n_pump_groups, S.n_pot = P.n_potential_groups, S.n_pulse = P.n_pulse_groups;
+        S.plane = plane;
+        for (int q = 0; q < comps; ++q) {
+            S.pump[q] = rplane(pump[q]);
+            S.pot[q] = rplane(pot[q]);
+            S.pulse[q] = cplane(pulse[q]);
+        }
+        // the envelopes' amplitudes at t (amp, not interpolated)
+        for (int g = 0; g < P.n_pump_groups; ++g) S.amp_pump[g] = mk_host(amp_pump[g]);
+        for (int g = 0; g < P.n_potential_groups; ++g) S.amp_pot[g] = mk_host(amp_pot[g]);
+        for (int g = 0; g < P.n_pulse_groups; ++g) S.amp_pulse[g] = mk_host(amp_pulse[g]);
+        const StageParams<T> B = base_params(0);
+        S.noise = B.noise;
+        S.noise_amp = B.noise_amp;
+        S.periodic_x = P.periodic_x, S.periodic_y = P.periodic_y;
+        const int blocks = (int)std::min<long long>((N + 255) / 256, 148 * 16);
+        C* w[2] = {reinterpret_cast<C*>(ssfm_w[0].p), comps > 1 ? reinterpret_cast<C*>(ssfm_w[1].p) : nullptr};
+        C* f[2] = {reinterpret_cast<C*>(ssfm_f[0].p), comps > 1 ? reinterpret_cast<C*>(ssfm_f[1].p) : nullptr};
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        for (int q = 0; q < comps; ++q)
+            gather_interior_kernel<T><<<blocks, 256, 0, stream>>>(cplane(psi[q]), pitch, N_r, N_c, w[q]);
+        for (int half = 0; half < 2; ++half) {
+            for (int q = 0; q < comps; ++q) {
+                ssfm_fft(w[q], f[q], CUFFT_FORWARD);
+                ssfm_linear_kernel<T><<<blocks, 256, 0, stream>>>(S, f[q], w[q]);
+                ssfm_fft(w[q], f[q], CUFFT_INVERSE);
+            }
+            if (half == 1) break;
+            T* rvm = comps > 1 ? rplane(nres[1]) : nullptr;
+            T* brvm = comps > 1 ? rplane(sbuf_n[1][0]) : nullptr;
+            ssfm_nonlinear_kernel<T><<<blocks, 256, 0, stream>>>(S, f[0], f[1], rplane(nres[0]), rvm, w[0], w[1],
+                                                                 rplane(sbuf_n[0][0]), brvm);
+        }
+        ssfm_independent_kernel<T><<<blocks, 256, 0, stream>>>(S, f[0], f[1], rplane(nres[0]), rplane(sbuf_n[0][0]),
+                                                               comps > 1 ? rplane(sbuf_n[1][0]) : nullptr, cplane(psi[0]),
+                                                               comps > 1 ? cplane(psi[1]) : nullptr);
+        prof_end(PHX_KERNEL_OTHER, a, (double)N * comps * 16 * sizeof(C));
+        launches += comps * 3 + 2;
+        PHX_CUDA(cudaGetLastError());
+    }
+
     // ------------------------------------------------------------ FFT filter
     void fft_filter() {
         for (int q = 0; q < comps; ++q) {
@@ -1119,6 +1196,8 @@ struct Engine final : EngineBase {
             }
             if (P.iterator == PHX_ITER_RK4) {
                 step_rk4();
+            } else if (P.iterator == PHX_ITER_SSFM) {
+                step_ssfm();
             } else if (tab.adaptive) {
                 step_adaptive(P.adaptive != 0, acc, rej);
             } else {
@@ -1560,10 +1639,11 @@ void validate(const phx_params& p) {
     if ((long long)p.N_c * p.N_r > (1LL << 31)) fail(PHX_ERR_INVALID_ARG, "grid too large");
     if (p.dtype != PHX_F32 && p.dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "dtype must be PHX_F32 or PHX_F64");
     if (p.dtype == PHX_F32 && (p.N_c & 1)) fail(PHX_ERR_UNSUPPORTED, "FP32 grids need an even N_c");
-    if (p.iterator < PHX_ITER_RK4 || p.iterator > PHX_ITER_NSRK78) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
+    if (p.iterator < PHX_ITER_RK4 || p.iterator > PHX_ITER_SSFM) fail(PHX_ERR_INVALID_ARG, "unknown iterator");
     {
         phx::Tableau t;
-        if (p.adaptive && (p.iterator == PHX_ITER_RK4 || !phx::tableau_resolve(p.iterator, t) || !t.adaptive))
+        if (p.adaptive && (p.iterator == PHX_ITER_RK4 || p.iterator == PHX_ITER_SSFM || !phx::tableau_resolve(p.iterator, t) ||
+                           !t.adaptive))
             fail(PHX_ERR_INVALID_ARG, "adaptive stepping needs an adaptive iterator (DP45, BoSha, CashKarp, Fehlberg2, "
                                       "Fehlberg5, DP85, NSRK78)");
     }

@@ -332,6 +332,7 @@ class SolverFactory:
         "FEHLBERG5": (True, "Fehlberg 5(4) order method for time integration."),
         "DP85": (True, "Dormand–Prince 8(5) method for time integration."),
         "NSRK78": (True, "Nullspace RK 13-stage 8th order"),
+        "SSFM": (False, "Split Step Fourier Method"),
     }
 
     @classmethod
