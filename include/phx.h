@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define PHX_ABI_VERSION 1
+#define PHX_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PHX_API __attribute__((visibility("default")))
@@ -78,9 +78,11 @@ typedef enum {
     PHX_ITER_SSFM = 20      /* "SSFM"      split_step_fourier_method.cu:74 (split-step Fourier, periodic) */
 } phx_iterator;
 
-/* DP45 error norm.  PHX_NORM_REFERENCE reproduces the reference's sums over
- * halo-padded subgrids of a single subgrid (cuda_matrix.cuh:614-632,699-705,
- * solver.cu:73-75); PHX_NORM_INTERIOR sums over grid points only. */
+/* Norms of the adaptive error control and of the imaginary-time
+ * normalisation.  PHX_NORM_REFERENCE reproduces the reference's sums over
+ * the halo-padded buffer of a single subgrid (cuda_matrix.cuh:614-632,699-705,
+ * solver.cu:73-75, solver_normalize_imag_time.cu:14-25); PHX_NORM_INTERIOR
+ * sums over grid points only. */
 typedef enum { PHX_NORM_REFERENCE = 0, PHX_NORM_INTERIOR = 1 } phx_norm_mode;
 
 /* Fields of MatrixContainer (include/solver/matrix_container.cuh:16-53) that
@@ -124,7 +126,7 @@ typedef struct {
     int32_t dtype;                  /* phx_dtype: the build precision of the reference */
     int32_t iterator;               /* phx_iterator */
     int32_t adaptive;               /* -adaptive (DP45) */
-    int32_t norm_mode;              /* phx_norm_mode (DP45 only) */
+    int32_t norm_mode;              /* phx_norm_mode (adaptive error, imaginary-time norm) */
     double dt, t0, t_max;           /* --dt, --t0, --tmax */
     double tol, dt_min, dt_max;     /* --tol, --rkvdt */
     double fft_every;               /* --fftEvery (ps) */
@@ -132,6 +134,11 @@ typedef struct {
     uint64_t seed;                  /* noise seed */
     int32_t n_pump_groups, n_potential_groups, n_pulse_groups;
     int32_t device;                 /* CUDA device ordinal */
+    double imag_time_amplitude;     /* --imagTime A: imaginary-time propagation (complex step
+                                       (0, -dt) in every stage sum, then every field scaled to
+                                       sum |f|^2 dV = A after each iteration); 0 = real time.
+                                       Runge-Kutta iterators need use_reservoir = 0 (the complex
+                                       step makes the reservoir complex); SSFM takes both */
 } phx_params;
 
 typedef struct {

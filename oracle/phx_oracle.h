@@ -81,6 +81,7 @@ typedef struct {
     phx_oracle_temporal pulse_t[PHX_ORACLE_MAX_GROUPS];
     double stochastic_amplitude; /* --dw; noise is on when > 0 */
     uint64_t seed;
+    double imag_time_amplitude;  /* --imagTime; imaginary-time propagation when != 0 */
 } phx_oracle_params;
 
 /* Derived kernel constants as calculateAuto computes them (system.cpp:116-160),

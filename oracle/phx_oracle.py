@@ -41,6 +41,7 @@ class Params(C.Structure):
         ("fft_every", C.c_double), ("use_fft_mask", C.c_int32), ("n_pump", C.c_int32), ("n_potential", C.c_int32),
         ("n_pulse", C.c_int32), ("pump_t", Temporal * MAX_GROUPS), ("potential_t", Temporal * MAX_GROUPS),
         ("pulse_t", Temporal * MAX_GROUPS), ("stochastic_amplitude", C.c_double), ("seed", C.c_uint64),
+        ("imag_time_amplitude", C.c_double),
     ]
 
 
@@ -103,6 +104,7 @@ def make_params(case):
     p.use_fft_mask = int(bool(case.get("mask_cut")))
     p.stochastic_amplitude = float(case.get("dw", 0.0))
     p.seed = int(case.get("seed", 0))
+    p.imag_time_amplitude = float(case.get("imag_time", 0.0))
     p.n_pump, p.n_potential, p.n_pulse = npump, len(case.get("potentials", [])), len(case.get("pulses", []))
     for fam, n in (("pump", p.n_pump), ("potential", p.n_potential), ("pulse", p.n_pulse)):
         specs = case.get(f"{fam}_t", [None] * n)

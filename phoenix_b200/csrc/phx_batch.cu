@@ -474,6 +474,7 @@ void validate_batch(const phx_params* ps, int n) {
         if (p.device != ps[0].device) fail(PHX_ERR_INVALID_ARG, at + "all instances share one device");
         if (p.iterator != PHX_ITER_RK4 || p.adaptive) fail(PHX_ERR_UNSUPPORTED, at + "batches run fixed-step RK4");
         if (p.tetm) fail(PHX_ERR_UNSUPPORTED, at + "batches run the scalar model");
+        if (p.imag_time_amplitude != 0.0) fail(PHX_ERR_UNSUPPORTED, at + "batches run real time");
         if (p.n_pump_groups > 1 || p.n_potential_groups > 1 || p.n_pulse_groups != 0)
             fail(PHX_ERR_UNSUPPORTED, at + "batch instances take at most one pump and one potential group and no pulse");
         if (p.n_pump_groups < 0 || p.n_potential_groups < 0) fail(PHX_ERR_INVALID_ARG, at + "negative group count");

@@ -119,6 +119,10 @@ inline bool tableau_for(int it, Tableau& t) {
         t.S = S, t.H = H, t.adaptive = true, t.fsal = fsal, t.power = power;
     };
     switch (it) {
+        case PHX_ITER_RK4:  // runge_kutta.cu:74-94 (the k-stack form; real-time RK4 runs the fused iteration)
+            cs({0.0, 0.5, 0.5, 1.0});
+            row(0, {0.5}), row(1, {0.5}), row(2, {1.0}), fin({1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0});
+            return true;
         case PHX_ITER_RK3:  // runge_kutta.cu:33-47
             cs({0.0, 1.0 / 2.0, 1.0});
             row(0, {0.5}), row(1, {-1.0, 2.0}), fin({1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0});

@@ -130,7 +130,14 @@ struct RingParams {
     NoiseParams noise;
     T noise_amp, w_sum[kMaxStages], R, gamma_c, four_dV, noise_scale;
     const T* n0;       // state reservoir, or nullptr without reservoir
+    int imag;          // imaginary time: the sums' complex step (0, -dt), as in the stage kernels
+    T dtw_final;       // final_ring_kernel: dt * b_1 for a one-weight final sum
 };
+
+template <typename T>
+__device__ __forceinline__ cx<T> ring_inc(const RingParams<T>& R, cx<T> v) {
+    return R.imag ? mi(v) : v;
+}
 
 template <typename T>
 __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
@@ -167,7 +174,7 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
         const cx<T> y0 = R.psi0[idx];
         cx<T> y;
         if (m == 1) {
-            y = cadd(y0, smul(R.dtw1, R.k[idx]));
+            y = cadd(y0, ring_inc(R, smul(R.dtw1, R.k[idx])));
         } else {
             // as the stage kernels: up to 7 weights left to right, more nested from the right
             const int n = R.nw[m - 1];
@@ -181,7 +188,7 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
                 acc = !have ? tq : (wide ? cadd(tq, acc) : cadd(acc, tq));
                 have = true;
             }
-            y = cadd(y0, smul(R.dt, acc));
+            y = cadd(y0, ring_inc(R, smul(R.dt, acc)));
         }
         if (R.noise.on) {
             const cx<T> xi = noise_xi(R.noise, noise_point(r, c, R.N_r, R.N_c, R.periodic_x, R.periodic_y), R.noise_amp);
@@ -210,6 +217,109 @@ __global__ void dp45_ring_kernel(const __grid_constant__ RingParams<T> R) {
         R.partials[2 * blockIdx.x] = a;
         R.partials[2 * blockIdx.x + 1] = b;
     }
+}
+
+// The halo rings 1..H of the state after an in-place final sum
+// (FINAL_SUM_K over the whole padded subgrid, cuda_macro.cuh:200-229), for
+// the imaginary-time normalisation over the padded buffer
+// (solver_normalize_imag_time.cu:14-25).  A cell at ring distance rho holds
+// y0 + dt sum_q b_q k_q with only k_1..k_{H-rho} ever computed there (the
+// others stay zero, so they add nothing), plus the dw term; y0 is the
+// synchronised halo of the step's start (images along periodic axes, zero
+// outside a zero axis), read from the state before the final sum replaces
+// it.  Rows: R.a[R.S - 1] / R.nw[R.S - 1] hold the final weights.
+// Per-block partials (norm, 0).
+template <typename T>
+__global__ void final_ring_kernel(const __grid_constant__ RingParams<T> R) {
+    const int B = R.H;
+    const long long W = R.N_c + 2LL * B;
+    const long long band_tb = (long long)B * W, band_lr = (long long)R.N_r * B;
+    const long long total = 2 * band_tb + 2 * band_lr;
+    const int m = R.S;  // the final sum's row
+    const int n = R.nw[m - 1];
+    double nrm = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int r, c;
+        if (t < 2 * band_tb) {
+            const long long u = t % band_tb;
+            r = (t < band_tb ? -B : R.N_r) + (int)(u / W);
+            c = (int)(u % W) - B;
+        } else {
+            const long long u = (t - 2 * band_tb) % band_lr;
+            r = (int)(u / B);
+            c = ((t - 2 * band_tb) < band_lr ? -B : R.N_c) + (int)(u % B);
+        }
+        const int dr = r < 0 ? -r : (r >= R.N_r ? r - R.N_r + 1 : 0);
+        const int dc = c < 0 ? -c : (c >= R.N_c ? c - R.N_c + 1 : 0);
+        const int rho = max(dr, dc);
+        const int sr = (dr && R.periodic_y) ? (r + R.N_r) % R.N_r : r;
+        const int sc = (dc && R.periodic_x) ? (c + R.N_c) % R.N_c : c;
+        const long long idx = (long long)sr * R.pitch + sc;
+        const int kv = min(n, R.H - rho);  // weights whose k exists here
+        cx<T> y = R.psi0[idx];
+        if (n == 1) {
+            if (kv >= 1) y = cadd(y, ring_inc(R, smul(R.dtw_final, R.k[idx])));
+        } else if (kv >= 1) {
+            const bool wide = n > 7;
+            cx<T> acc = mk((T)0, (T)0);
+            bool have = false;
+            for (int u = 0; u < kv; ++u) {
+                const int q = wide ? kv - 1 - u : u;
+                if (wide && R.a[m - 1][q] == (T)0) continue;
+                const cx<T> tq = smul(R.a[m - 1][q], R.k[(long long)q * R.plane + idx]);
+                acc = !have ? tq : (wide ? cadd(tq, acc) : cadd(acc, tq));
+                have = true;
+            }
+            if (have) y = cadd(y, ring_inc(R, smul(R.dt, acc)));
+        }
+        if (R.noise.on) {
+            const cx<T> xi = noise_xi(R.noise, noise_point(r, c, R.N_r, R.N_c, R.periodic_x, R.periodic_y), R.noise_amp);
+            const T s_ = R.n0 ? rsqrt_rn(rdiv(radd(rmul(R.R, R.n0[idx]), R.gamma_c), R.four_dV)) : R.noise_scale;
+            y = cadd(y, mk(rmul(rmul(R.w_sum[m - 1], xi.re), s_), rmul(rmul(R.w_sum[m - 1], xi.im), s_)));
+        }
+        nrm += (double)abs2(y);
+    }
+    for (int o = 16; o > 0; o >>= 1) nrm += __shfl_down_sync(0xffffffffu, nrm, o);
+    __shared__ double s[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s[warp] = nrm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) a += s[w];
+        R.partials[2 * blockIdx.x] = a;
+        R.partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// Imaginary-time factor sqrt(A / (s dV)) of one field, s = the sum of the
+// first slots of n partial pairs rounded to T, 1 when below 1e-10
+// (solver_normalize_imag_time.cu:18-25).  One block.
+template <typename T>
+__global__ void imag_factor_kernel(const double* __restrict__ partials, long long n, T A, T dV, T* __restrict__ factor) {
+    __shared__ double s[32];
+    double a = 0.0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) a += partials[2 * i];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s[warp] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) v += s[w];
+        T sum = (T)v;
+        if ((double)sum < 1e-10) sum = (T)1.0;
+        *factor = rsqrt_rn(rdiv(A, rmul(sum, dV)));
+    }
+}
+
+// every element of a padded plane (n values of T; a complex plane as 2 n)
+// times the factor: complex * real is (re f, im f)
+template <typename T>
+__global__ void scale_plane_kernel(T* __restrict__ base, long long n, const T* __restrict__ factor, T host_factor) {
+    const T f = factor ? *factor : host_factor;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        base[i] = rmul(base[i], f);
 }
 
 // Outer ring (rho == H) of the state's synchronised halo: images along

@@ -118,6 +118,12 @@ struct Engine final : EngineBase {
     int tune_step = 0;              // steps run while tuning
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 5];
     static constexpr int kRingBlocks = 64;
+    static constexpr int kNormBlocks = 296;
+    // imaginary-time propagation (--imagTime): k-stack sums with the complex
+    // step, then Solver::normalizeImaginaryTimePropagation after every iteration
+    bool imag_time() const { return P.imag_time_amplitude != 0.0; }
+    DevBuf imag_f;           // the device-side normalisation factor (T)
+    double imag_nrm = 0.0;   // adaptive stepping: the accepted attempt's norm
     using C = cx<T>;
 
     int N_r = 0, N_c = 0;
@@ -173,6 +179,8 @@ struct Engine final : EngineBase {
         comps = P.tetm ? 2 : 1;
         if (P.iterator != PHX_ITER_RK4 && P.iterator != PHX_ITER_SSFM && !tableau_resolve(P.iterator, tab))
             fail(PHX_ERR_INVALID_ARG, "unknown iterator");
+        // imaginary-time RK4 runs the k-stack stage kernels (complex step)
+        if (P.iterator == PHX_ITER_RK4 && imag_time()) tableau_resolve(PHX_ITER_RK4, tab);
         // halo_size_ = k_max_ of the iterator's constructor (SSFM: 0); the ring holds it
         H = P.iterator == PHX_ITER_RK4 ? 4 : (P.iterator == PHX_ITER_SSFM ? 0 : tab.H);
         G = std::max(kRing, H + 1);
@@ -190,7 +198,7 @@ struct Engine final : EngineBase {
                 sbuf_psi[q][b].alloc(cb, stream);
                 sbuf_n[q][b].alloc(rb, stream);
             }
-            if (P.iterator == PHX_ITER_RK4) {
+            if (P.iterator == PHX_ITER_RK4 && !imag_time()) {
                 acc_psi[q].alloc(cb, stream);
                 acc_n[q].alloc(rb, stream);
             } else {
@@ -213,6 +221,7 @@ struct Engine final : EngineBase {
         partials.alloc(sizeof(double) * 2 * std::max<long long>(max_blocks, 1024), stream);
         result.alloc(sizeof(double) * 4, stream);
         host_result.alloc(sizeof(double) * 4);
+        imag_f.alloc(sizeof(double) * 2, stream);
         t = (T)P.t0;
         dt = (T)P.dt;
         fft_cached_t = (T)0.0;
@@ -230,7 +239,7 @@ struct Engine final : EngineBase {
     // every iteration)
     bool fused_eligible_static() const {
         return P.iterator == PHX_ITER_RK4 && !P.tetm && P.n_pump_groups <= 1 && P.n_potential_groups <= 1 &&
-               P.n_pulse_groups == 0 && !(P.stochastic_amplitude > 0.0);
+               P.n_pulse_groups == 0 && !(P.stochastic_amplitude > 0.0) && !imag_time();
     }
     long long rows_per_block(int sh) const { return (long long)kShapeRB[sh] * kShapeWarps[sh]; }
     long long grid_y(long long r0, long long r1) const {
@@ -443,6 +452,7 @@ struct Engine final : EngineBase {
         S.four_dV = (T)4.0 * d.dV;
         S.gamma_c = (T)P.gamma_c;
         S.noise_scale = std::sqrt((T)P.gamma_c / S.four_dV);
+        S.imag = imag_time() ? 1 : 0;
         return S;
     }
     // weight sum of a stage sum's dw term: the right fold w_1 + (w_2 + (...))
@@ -767,37 +777,111 @@ struct Engine final : EngineBase {
     // the state in place (CALCULATE_K / INTERMEDIATE_SUM_K / FINAL_SUM_K).
     void step_tableau() {
         // a one-stage method (Newton) reads its stencil from the state, so its
-        // sum goes to a stage plane that then becomes the state
+        // sum goes to a stage plane that then becomes the state; so does every
+        // final sum in imaginary time, whose normalisation reads the state of
+        // the step's start
         const bool single = tab.S == 1;
+        const bool imag = imag_time();
+        const bool to_buf = single || imag;
+        // reference norm: the final stage also covers the rings where its k
+        // exists (H - S), as CALCULATE_K does there
+        const bool ring = imag && P.norm_mode == PHX_NORM_REFERENCE;
         for (int s = 1; s <= tab.S; ++s) {
             const bool last = s == tab.S;
             StageParams<T> S = base_params(0);
             set_coefficients(S, (T)tab.c[s - 1]);
-            region(S, last ? 0 : H - s);
+            region(S, last ? (ring ? std::max(0, H - s) : 0) : H - s);
             S.stage = s;
             S.nw = last ? tab.nb : tab.nw[s - 1];
             for (int q = 0; q < S.nw; ++q) S.w[q] = (T)(last ? tab.b[q] : tab.a[s - 1][q]);
             if (S.nw == 1) S.dtw = dt * S.w[0];
             S.w_sum = right_fold(S.w, S.nw);
-            auto wire = [this, s, last, single](StageParams<T>& X, int q) {
+            auto wire = [this, s, last, to_buf](StageParams<T>& X, int q) {
                 X.psi0 = cplane(psi[q]);
                 X.n0 = rplane(nres[q]);
                 X.psi_in = s == 1 ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 2) & 1]);
                 X.n_in = s == 1 ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 2) & 1]);
                 X.k_psi = cplane(k_psi[q]);
                 X.k_n = rplane(k_n[q]);
-                X.psi_out = last && !single ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 1) & 1]);
-                X.n_out = last && !single ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 1) & 1]);
+                X.psi_out = last && !to_buf ? cplane(psi[q]) : cplane(sbuf_psi[q][(s - 1) & 1]);
+                X.n_out = last && !to_buf ? rplane(nres[q]) : rplane(sbuf_n[q][(s - 1) & 1]);
                 X.pump = rplane(pump[q]);
                 X.pot = rplane(pot[q]);
                 X.pulse = cplane(pulse[q]);
             };
-            if (last)
+            if (last && !ring)
                 launch<kStackFinal>(S, wire);
             else
                 launch<kStack>(S, wire);
         }
-        if (single) swap_state_with(0);
+        if (!imag) {
+            if (single) swap_state_with(0);
+            return;
+        }
+        long long nb = kNormBlocks;
+        if (ring) {
+            // the halo rings of the reference's buffer after its in-place final
+            // sum, from the state of the step's start and the k-stack
+            RingParams<T> R;
+            std::memset(&R, 0, sizeof(R));
+            R.psi0 = cplane(psi[0]);
+            R.k = cplane(k_psi[0]);
+            R.pitch = pitch;
+            R.plane = plane;
+            R.N_r = N_r;
+            R.N_c = N_c;
+            R.periodic_x = P.periodic_x;
+            R.periodic_y = P.periodic_y;
+            R.H = H;
+            R.S = tab.S;
+            R.dt = dt;
+            R.nw[tab.S - 1] = tab.nb;
+            for (int q = 0; q < tab.nb; ++q) R.a[tab.S - 1][q] = (T)tab.b[q];
+            R.dtw_final = dt * (T)tab.b[0];
+            const StageParams<T> B = base_params(0);
+            R.noise = B.noise;
+            R.noise_amp = B.noise_amp;
+            R.w_sum[tab.S - 1] = right_fold(R.a[tab.S - 1], tab.nb);
+            R.R = B.R;
+            R.gamma_c = B.gamma_c;
+            R.four_dV = B.four_dV;
+            R.noise_scale = B.noise_scale;
+            R.n0 = nullptr;
+            R.imag = 1;
+            R.partials = reinterpret_cast<double*>(partials.p) + 2 * kNormBlocks;
+            final_ring_kernel<T><<<kRingBlocks, 256, 0, stream>>>(R);
+            ++launches;
+            PHX_CUDA(cudaGetLastError());
+            nb += kRingBlocks;
+        }
+        swap_state_with((tab.S - 1) & 1);
+        imag_normalize_device(psi[0], true, nb);
+    }
+
+    // Solver::normalizeImaginaryTimePropagation (solver_normalize_imag_time.cu:12-48)
+    // for one field: the interior sum (FP64 partials, plus `nb - kNormBlocks`
+    // ring partials already in place), the factor on the device, and the
+    // whole padded plane scaled by it
+    void imag_normalize_device(DevBuf& f, bool complex_field, long long nb) {
+        double* pp = reinterpret_cast<double*>(partials.p);
+        if (complex_field)
+            sum_abs2_kernel<T, true><<<kNormBlocks, 256, 0, stream>>>(reinterpret_cast<const T*>(cplane(f)), pitch, N_r, N_c, pp);
+        else
+            sum_abs2_kernel<T, false><<<kNormBlocks, 256, 0, stream>>>(rplane(f), pitch, N_r, N_c, pp);
+        imag_factor_kernel<T><<<1, 1024, 0, stream>>>(pp, nb, (T)P.imag_time_amplitude, d.dV, reinterpret_cast<T*>(imag_f.p));
+        scale_plane_kernel<T><<<kNormBlocks, 256, 0, stream>>>(reinterpret_cast<T*>(f.p), (complex_field ? 2 : 1) * plane,
+                                                               reinterpret_cast<const T*>(imag_f.p), (T)0);
+        launches += 3;
+        PHX_CUDA(cudaGetLastError());
+    }
+    // adaptive stepping: the accepted attempt's norm is the state's norm
+    void imag_normalize_host(DevBuf& f, double norm) {
+        T sum = (T)norm;
+        if ((double)sum < 1e-10) sum = (T)1.0;
+        const T fac = std::sqrt((T)P.imag_time_amplitude / (sum * d.dV));
+        scale_plane_kernel<T><<<kNormBlocks, 256, 0, stream>>>(reinterpret_cast<T*>(f.p), 2 * plane, nullptr, fac);
+        ++launches;
+        PHX_CUDA(cudaGetLastError());
     }
 
     // ------------------------------------------------------------ adaptive tableaux
@@ -885,6 +969,7 @@ struct Engine final : EngineBase {
             R.E = tab.E;
             for (int q = 0; q < tab.E; ++q) R.e[q] = (T)tab.e[q];
             R.passes = P.tetm ? 2 : 1;
+            R.imag = imag_time() ? 1 : 0;
             R.partials = reinterpret_cast<double*>(partials.p) + 2 * nb;
             {
                 const StageParams<T> B = base_params(0);
@@ -981,6 +1066,7 @@ struct Engine final : EngineBase {
             if (accept) {
                 swap_state_with(sol_slot());
                 r7_prev = r7_cur;
+                imag_nrm = nrm;
                 ++acc;
             } else {
                 ++rej;
@@ -1194,14 +1280,25 @@ struct Engine final : EngineBase {
                 ta = get_event();
                 PHX_CUDA(cudaEventRecord(ta, stream));
             }
-            if (P.iterator == PHX_ITER_RK4) {
+            if (P.iterator == PHX_ITER_RK4 && !imag_time()) {
                 step_rk4();
             } else if (P.iterator == PHX_ITER_SSFM) {
                 step_ssfm();
-            } else if (tab.adaptive) {
+            } else if (tab.adaptive && !(imag_time() && !P.adaptive)) {
                 step_adaptive(P.adaptive != 0, acc, rej);
             } else {
-                step_tableau();
+                step_tableau();  // imaginary time: normalised inside
+            }
+            if (imag_time()) {
+                if (P.iterator == PHX_ITER_SSFM) {
+                    // halo 0: the sums run over the grid points
+                    for (int q = 0; q < comps; ++q) {
+                        imag_normalize_device(psi[q], true, kNormBlocks);
+                        if (P.use_reservoir) imag_normalize_device(nres[q], false, kNormBlocks);
+                    }
+                } else if (tab.adaptive && P.adaptive) {
+                    imag_normalize_host(psi[0], imag_nrm);
+                }
             }
             if (shape < 0) tune_record(ta, tb);
             ++its;
@@ -1307,6 +1404,7 @@ struct Engine final : EngineBase {
         if (P.iterator != PHX_ITER_RK4 || P.tetm) fail(PHX_ERR_UNSUPPORTED, "the adjoint covers scalar fixed-step RK4");
         if (!P.periodic_x || !P.periodic_y) fail(PHX_ERR_UNSUPPORTED, "the adjoint needs periodic boundaries on both axes");
         if (P.stochastic_amplitude > 0.0) fail(PHX_ERR_UNSUPPORTED, "the adjoint of a noisy run is not defined here");
+        if (imag_time()) fail(PHX_ERR_UNSUPPORTED, "the adjoint covers real-time RK4");
         if (have_mask[0] || have_mask[1]) fail(PHX_ERR_UNSUPPORTED, "the adjoint does not cover the k-space filter");
         if (P.n_pump_groups > 1 || P.n_potential_groups > 1 || P.n_pulse_groups != 0)
             fail(PHX_ERR_UNSUPPORTED, "the adjoint takes at most one pump and one potential group and no pulse");
@@ -1655,6 +1753,15 @@ void validate(const phx_params& p) {
         fail(PHX_ERR_INVALID_ARG, "temporal group count out of range (0..8)");
     if (p.n_pump_groups > 0 && !p.use_reservoir) fail(PHX_ERR_INVALID_ARG, "pump groups need use_reservoir");
     if (p.tetm && !p.use_reservoir) fail(PHX_ERR_UNSUPPORTED, "TE/TM mode reads the reservoir; set use_reservoir");
+    if (!std::isfinite(p.imag_time_amplitude)) fail(PHX_ERR_INVALID_ARG, "imag_time_amplitude must be finite");
+    if (p.imag_time_amplitude != 0.0) {
+        if (p.use_reservoir && p.iterator != PHX_ITER_SSFM)
+            fail(PHX_ERR_UNSUPPORTED, "imaginary time with a reservoir: the complex step makes the reservoir complex, "
+                                      "which this library stores real (SSFM keeps it real and is supported)");
+        if (p.iterator == PHX_ITER_DP85)
+            fail(PHX_ERR_UNSUPPORTED, "imaginary time is not provided for DP85 (its reference step swaps the fixed and "
+                                      "variable branches)");
+    }
     if (!std::isfinite(p.stochastic_amplitude)) fail(PHX_ERR_INVALID_ARG, "stochastic_amplitude must be finite");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

@@ -78,7 +78,18 @@ struct StageParams {
     T dV, four_dV;       // dV, 4 dV
     T gamma_c;
     T noise_scale;       // sqrt(gamma_c / (4 dV)), the scale without reservoir
+    // imaginary time (--imagTime): the k-stack sums take the complex step
+    // (0, -dt): ((0, -dt) w) k = -i (dt w) k and (0, -dt) a = -i (dt a),
+    // the same bits as the complex products of the complex_dt branches
+    // (kernel_summation.cuh:66-190) up to the sign of an exact zero; the
+    // wavefunction only (no reservoir runs with it)
+    int imag;
 };
+
+template <typename T>
+__device__ __forceinline__ cx<T> step_inc(const StageParams<T>& P, cx<T> v) {
+    return P.imag ? mi(v) : v;
+}
 
 // ---- 16-byte packs: CPT grid points per lane ----
 template <typename T>
@@ -366,7 +377,7 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
 #pragma unroll
                         for (int j = 0; j < CPT; ++j) {
                             if (P.nw == 1) {
-                                out_wf.v[j] = cadd(y0.v[j], smul(P.dtw, out_wf.v[j]));
+                                out_wf.v[j] = cadd(y0.v[j], step_inc(P, smul(P.dtw, out_wf.v[j])));
                                 if constexpr (RES) out_rv.v[j] = radd(n0.v[j], rmul(P.dtw, out_rv.v[j]));
                             } else {
                                 // up to 7 weights: left to right, zeros included
@@ -398,7 +409,7 @@ __global__ void __launch_bounds__(32 * WARPS) stage_scalar_kernel(const __grid_c
                                         a = cadd(a, tq), an = radd(an, tn);
                                     }
                                 }
-                                out_wf.v[j] = cadd(y0.v[j], smul(P.dt, a));
+                                out_wf.v[j] = cadd(y0.v[j], step_inc(P, smul(P.dt, a)));
                                 if constexpr (RES) out_rv.v[j] = radd(n0.v[j], rmul(P.dt, an));
                             }
                             if (P.noise.on) {

@@ -61,10 +61,11 @@ class SystemParameters:
     pump_temporal: List[Temporal] = field(default_factory=list)
     potential_temporal: List[Temporal] = field(default_factory=list)
     pulse_temporal: List[Temporal] = field(default_factory=list)
-    norm_mode: str = "reference"  # DP45 error norm: "reference" (halo-padded sums) or "interior"
+    norm_mode: str = "reference"  # adaptive error / imaginary-time norm: "reference" (halo-padded sums) or "interior"
     stochastic_amplitude: float = 0.0  # --dw; noise is on when > 0
     random_seed: int = 0  # key of the counter-based noise generator
     device: int = 0
+    imag_time_amplitude: float = 0.0  # --imagTime A; imaginary-time propagation when != 0
 
     def magic_timestep(self) -> float:
         dx = self.L_x / (self.N_c - 1)
@@ -96,6 +97,7 @@ class SystemParameters:
         p.fft_every = float(self.fft_every)
         p.stochastic_amplitude = float(self.stochastic_amplitude)
         p.seed = int(self.random_seed) & 0xFFFFFFFFFFFFFFFF
+        p.imag_time_amplitude = float(self.imag_time_amplitude)
         p.n_pump_groups = len(self.pump_temporal)
         p.n_potential_groups = len(self.potential_temporal)
         p.n_pulse_groups = len(self.pulse_temporal)
@@ -371,6 +373,7 @@ def system_from_case(case: dict, **overrides) -> SystemParameters:
         dt_min=case.get("dt_min", 1e-4), dt_max=case.get("dt_max", 3.0), fft_every=case.get("fft_every", 1e9),
         t0=case.get("t0", 0.0), t_max=case["t_max"], dt=case["dt"],
         stochastic_amplitude=case.get("dw", 0.0), random_seed=case.get("seed", 0),
+        imag_time_amplitude=case.get("imag_time", 0.0),
         pump_temporal=temporal(case.get("pump_t"), npump),
         potential_temporal=temporal(case.get("potential_t"), len(case.get("potentials", []))),
         pulse_temporal=temporal(case.get("pulse_t"), len(case.get("pulses", []))))

@@ -118,6 +118,8 @@ def run_case(name, case):
             args += ["-adaptive", "--tol", repr(case["tol"]), "--rkvdt", repr(case["dt_min"]), repr(case["dt_max"])]
         if case.get("tetm"):
             args += ["-tetm"]
+        if case.get("imag_time"):
+            args += ["--imagTime", repr(case["imag_time"])]
         comps = ["plus", "minus"] if case.get("tetm") else ["plus"]
         for comp in comps:
             f = os.path.join(tmp, f"psi_{comp}.txt")
@@ -232,6 +234,26 @@ def cases():
     c["tab_ssprk3_f32_periodic"] = dict(grid, **STRONG, dtype="f32", iterator="SSPRK3", dt=0.005,
                                         t_max=20 * 0.005 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=43,
                                         psi_amp=1.0, pumps=[(4.0, 3.0, 0.0)], potentials=[0.2])
+    # imaginary-time propagation (--imagTime): complex step (0, -dt) in every
+    # stage sum, then every field scaled to sum |f|^2 dV = A over its padded
+    # buffer.  Without a reservoir (no pump, no initial reservoir) except the
+    # last case, where the complex step makes the reservoir complex.
+    im = dict(**STRONG, imag_time=2.5, psi_amp=1.0, potentials=[0.2])
+    c["imag_rk4_f64_periodic"] = dict(grid, **im, dtype="f64", iterator="RK4", dt=0.01,
+                                      t_max=20 * 0.01 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=61)
+    c["imag_rk4_f64_zero"] = dict(grid, **im, dtype="f64", iterator="RK4", dt=0.01, t_max=20 * 0.01 * (1 - 1e-9),
+                                  periodic_x=0, periodic_y=0, seed=62)
+    c["imag_rk4_f32_mixed"] = dict(N_c=40, N_r=32, L_x=25.0, L_y=20.0, **im, dtype="f32", iterator="RK4", dt=0.01,
+                                   t_max=20 * 0.01 * (1 - 1e-9), periodic_x=1, periodic_y=0, seed=63)
+    c["imag_heun3_f64_mixed"] = dict(N_c=40, N_r=32, L_x=25.0, L_y=20.0, **im, dtype="f64", iterator="Heun3",
+                                     dt=0.005, t_max=20 * 0.005 * (1 - 1e-9), periodic_x=0, periodic_y=1, seed=64)
+    c["imag_nsrk78_f64_zero"] = dict(grid, **im, dtype="f64", iterator="NSRK78", dt=0.01,
+                                     t_max=10 * 0.01 * (1 - 1e-9), periodic_x=0, periodic_y=0, seed=65)
+    c["imag_dp45_f64_adaptive"] = dict(grid, **im, dtype="f64", iterator="DP45", adaptive=1, tol=1e-6, dt_min=1e-5,
+                                       dt_max=0.05, dt=0.01, t_max=0.2, periodic_x=1, periodic_y=1, seed=66)
+    c["imag_rk4_f64_reservoir"] = dict(grid, **im, dtype="f64", iterator="RK4", dt=0.01,
+                                       t_max=10 * 0.01 * (1 - 1e-9), periodic_x=1, periodic_y=1, seed=67,
+                                       pumps=[(4.0, 3.0, 0.0)])
     return c
 
 

@@ -47,6 +47,21 @@ def test_create_rejects_bad_parameters_without_device_work():
     assert lib.phx_create(C.byref(p), C.byref(h)) == 6
 
 
+def test_imaginary_time_parameters_are_checked_without_device_work():
+    lib = L.load()
+    h = C.c_void_p()
+    # the complex step would make the reservoir complex: Runge-Kutta iterators refuse it
+    p = pb.SystemParameters(N_c=32, N_r=32, dt=0.01, imag_time_amplitude=1.0, use_reservoir=True).to_abi()
+    assert lib.phx_create(C.byref(p), C.byref(h)) == 6 and not h.value
+    assert b"reservoir" in lib.phx_last_error(None)
+    p = pb.SystemParameters(N_c=32, N_r=32, dt=0.01, imag_time_amplitude=1.0, use_reservoir=False,
+                            iterator="DP85").to_abi()
+    assert lib.phx_create(C.byref(p), C.byref(h)) == 6
+    p = pb.SystemParameters(N_c=32, N_r=32, dt=0.01, imag_time_amplitude=float("nan"), use_reservoir=False).to_abi()
+    assert lib.phx_create(C.byref(p), C.byref(h)) == 1
+    assert b"imag_time_amplitude" in lib.phx_last_error(None)
+
+
 def test_null_handle_calls_fail_cleanly():
     lib = L.load()
     assert lib.phx_step(None, 1, None) == 1
@@ -76,6 +91,8 @@ def test_batch_rejects_unsupported_instances_without_device_work():
         (pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f32", use_reservoir=True, use_twin_mode=True), 6, "scalar"),
         (pb.SystemParameters(N_c=63, N_r=64, dt=0.01, dtype="f32", use_reservoir=True), 6, "even"),
         (pb.SystemParameters(N_c=4, N_r=64, dt=0.01, dtype="f32", use_reservoir=True), 1, "8 x 8"),
+        (pb.SystemParameters(N_c=64, N_r=64, dt=0.01, dtype="f32", use_reservoir=True, imag_time_amplitude=1.0), 6,
+         "real time"),
     ]
     for bad, status, words in cases:
         st, msg = _batch_status([ok, bad])

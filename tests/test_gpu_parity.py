@@ -6,8 +6,9 @@ explicitly rounded operations in the reference's operand order, so FP64 and
 FP32 results are expected to be bit-identical to the reference CPU build;
 the asserted bounds are the north star's (rel-L2 <= 1e-12 for FP64) and
 1e-6 for FP32.  The k-space filter goes through cuFFT instead of FFTW, and
-DP45 sums its norms in FP64 instead of the build precision, so those cases
-are held to the bound, not to bit equality.
+DP45 and the imaginary-time normalisation sum their norms in FP64 instead
+of the build precision, so those cases are held to the bound, not to bit
+equality.
 """
 import glob
 import json
@@ -22,7 +23,9 @@ from oracle import phx_oracle as O
 pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
-SUPPORTED = GOLDEN
+# imaginary time with a reservoir makes the reservoir complex; the library
+# refuses it (PHX_ERR_UNSUPPORTED, tests/test_abi.py) and the oracle covers it
+SUPPORTED = [g for g in GOLDEN if os.path.basename(g) != "imag_rk4_f64_reservoir.npz"]
 
 
 def rel_l2(a, b):
@@ -62,7 +65,9 @@ def test_gpu_matches_reference_golden(require_gpu, path):
         ref = z[gk] if k.startswith("psi") else np.real(z[gk])
         err = rel_l2(out[k], ref)
         assert err <= tol, f"{k}: rel-L2 {err:.3e} > {tol}"
-        exact = not case.get("mask_cut") and not case.get("adaptive")
+        # the imaginary-time norm is summed in FP64 here, in the build precision
+        # (and another order) there: its factor agrees to rounding only
+        exact = not case.get("mask_cut") and not case.get("adaptive") and not case.get("imag_time")
         if exact:
             np.testing.assert_array_equal(out[k], ref, err_msg=f"{k} not bit-identical to the reference")
 
