@@ -53,7 +53,7 @@ typedef enum {
 typedef enum { PHX_F32 = 0, PHX_F64 = 1 } phx_dtype;
 
 /* iterator keys of REGISTER_SOLVER: "RK4" (runge_kutta.cu:96), "DP45" (dormand_prince.cu:97) */
-/* REGISTER_SOLVER keys of the reference (source/cuda_solver/solver/iterator/*.cu) */
+/* REGISTER_SOLVER keys of the reference (the .cu files of source/cuda_solver/solver/iterator) */
 typedef enum {
     PHX_ITER_RK4 = 0,       /* "RK4"      runge_kutta.cu:96 */
     PHX_ITER_DP45 = 1,      /* "DP45"     dormand_prince.cu:97 (adaptive) */
@@ -99,11 +99,20 @@ typedef enum {
     PHX_PULSE_PLUS = 8,      /* pulse_plus          complex, per group */
     PHX_PULSE_MINUS = 9,     /* pulse_minus         complex, per group */
     PHX_FFT_MASK_PLUS = 10,  /* fft_mask_plus       real, real-space order */
-    PHX_FFT_MASK_MINUS = 11  /* fft_mask_minus      real, real-space order */
+    PHX_FFT_MASK_MINUS = 11, /* fft_mask_minus      real, real-space order */
+    PHX_FFT_PLUS = 12,       /* fft_plus            complex, read only: the k-space field of the
+                                last filter time (phx_set_spectrum_output) */
+    PHX_FFT_MINUS = 13       /* fft_minus           complex, read only */
 } phx_field;
 
 /* Temporal envelope kinds (include/system/envelope.hpp:63-69,165-175) */
-typedef enum { PHX_TEMPORAL_CONSTANT = 0, PHX_TEMPORAL_IEXP = 1, PHX_TEMPORAL_COS = 2, PHX_TEMPORAL_GAUSS = 3 } phx_temporal_kind;
+typedef enum {
+    PHX_TEMPORAL_CONSTANT = 0,
+    PHX_TEMPORAL_IEXP = 1,
+    PHX_TEMPORAL_COS = 2,
+    PHX_TEMPORAL_GAUSS = 3,
+    PHX_TEMPORAL_LOADED = 4 /* a table of (t, re, im), phx_set_temporal_table */
+} phx_temporal_kind;
 
 /* Which temporal-envelope family a group belongs to */
 typedef enum { PHX_ENV_PUMP = 0, PHX_ENV_POTENTIAL = 1, PHX_ENV_PULSE = 2 } phx_envelope;
@@ -178,9 +187,29 @@ PHX_API phx_status phx_get_field(phx_handle* h, int32_t field, int32_t group, vo
 PHX_API phx_status phx_set_temporal(phx_handle* h, int32_t envelope, int32_t group, int32_t kind, double t0, double sigma,
                             double freq);
 
+/* A loaded temporal envelope (`time load <file>`, Envelope::addTemporal(path)
+ * and updateTemporal, envelope.cpp:106-120,472-489): the amplitude at t is
+ * interpolated linearly between the table's points (t ascending, n >= 2),
+ * and is the last value after the table's end.  Pump tables must be real. */
+PHX_API phx_status phx_set_temporal_table(phx_handle* h, int32_t envelope, int32_t group, const double* t,
+                                          const double* re, const double* im, int64_t n);
+
 /* Replaces the main loop's calls of Solver::iterate (main.cu:80-117,
  * solver.cu:22-70): run iterate() until t >= t_max or max_iterations calls. */
 PHX_API phx_status phx_step(phx_handle* h, int64_t max_iterations, phx_step_info* info);
+
+/* One Solver::iterate(force_fixed_time_step) call: info->iterations is 0 once
+ * t >= t_max.  force_fixed_time_step != 0 runs an adaptive iterator once with
+ * the current dt and no step-size control, as the main loop does for the
+ * step that lands on an output time (main.cu:86-101). */
+PHX_API phx_status phx_iterate(phx_handle* h, int32_t force_fixed_time_step, phx_step_info* info);
+
+/* Keep the k-space field of every fft_every time (Solver::applyFFTFilter,
+ * solver_fft.cu:67-100): the forward transform of psi, times mask / N where a
+ * mask is set, readable as PHX_FFT_PLUS / PHX_FFT_MINUS (N_r x N_c complex, the
+ * transform's own order).  Without a mask the transform is taken and psi is
+ * left as it is, as in the reference.  Off by default (no extra work). */
+PHX_API phx_status phx_set_spectrum_output(phx_handle* h, int32_t enable);
 
 /* Current t and dt (SystemParameters::p.t / p.dt). */
 PHX_API phx_status phx_get_time(phx_handle* h, double* t, double* dt);

@@ -68,6 +68,10 @@ _SIGS = {
     "phx_get_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),
     "phx_set_temporal": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "phx_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(StepInfo)]),
+    "phx_iterate": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(StepInfo)]),
+    "phx_set_temporal_table": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.c_int64]),
+    "phx_set_spectrum_output": (C.c_int, [C.c_void_p, C.c_int32]),
     "phx_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "phx_set_time": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     "phx_sum_abs2": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),

@@ -8,7 +8,9 @@
 #pragma once
 
 #include <cmath>
+#include <algorithm>
 #include <complex>
+#include <vector>
 #include <initializer_list>
 #include <cstdint>
 
@@ -39,12 +41,25 @@ Derived<T> derive(const phx_params& p) {
 struct TemporalSpec {
     int kind = PHX_TEMPORAL_CONSTANT;
     double t0 = 0, sigma = 0, freq = 0;
+    std::vector<double> tt, re, im;  // PHX_TEMPORAL_LOADED
 };
 
 template <typename T>
 std::complex<T> temporal_value(const TemporalSpec& s, T t) {
     const T t0 = (T)s.t0, sigma = (T)s.sigma, freq = (T)s.freq;
     switch (s.kind) {
+        case PHX_TEMPORAL_LOADED: {
+            // the table in the build precision: the last point after its end, else
+            // v1 + (v2 - v1) (t - t1) / (t2 - t1) between the neighbours of the
+            // first point >= t (index clamped to 1..n-1)
+            const size_t n = s.tt.size();
+            if (t > (T)s.tt[n - 1]) return std::complex<T>((T)s.re[n - 1], (T)s.im[n - 1]);
+            const auto it = std::lower_bound(s.tt.begin(), s.tt.end(), t, [](double a, T b) { return (T)a < b; });
+            const size_t idx = std::min<size_t>(std::max<size_t>(1, (size_t)(it - s.tt.begin())), n - 1);
+            const T t1 = (T)s.tt[idx - 1], t2 = (T)s.tt[idx];
+            const std::complex<T> v1((T)s.re[idx - 1], (T)s.im[idx - 1]), v2((T)s.re[idx], (T)s.im[idx]);
+            return v1 + (v2 - v1) * (t - t1) / (t2 - t1);
+        }
         case PHX_TEMPORAL_IEXP: {
             const T a = (t - t0) * (t - t0) / ((T)2.0 * sigma * sigma);
             const T b = freq * (t - t0);

@@ -44,7 +44,9 @@ struct EngineBase {
     int64_t launches = 0;
     std::string last_error;
     TemporalSpec pump_t[kMaxGroups], pot_t[kMaxGroups], pulse_t[kMaxGroups];
+    bool force_fixed = false;  // phx_iterate(force_fixed_time_step): no step-size control this call
     virtual ~EngineBase() = default;
+    virtual void set_spectrum_output(bool enable) = 0;
     virtual void init() = 0;
     virtual void set_field(int field, int group, const void* host, int64_t count, int dtype) = 0;
     virtual void get_field(int field, int group, void* host, int64_t count, int dtype) = 0;
@@ -122,6 +124,8 @@ struct Engine final : EngineBase {
     // imaginary-time propagation (--imagTime): k-stack sums with the complex
     // step, then Solver::normalizeImaginaryTimePropagation after every iteration
     bool imag_time() const { return P.imag_time_amplitude != 0.0; }
+    // step-size control this iteration (off for phx_iterate's forced fixed step)
+    bool adaptive_now() const { return P.adaptive != 0 && !force_fixed; }
     DevBuf imag_f;           // the device-side normalisation factor (T)
     double imag_nrm = 0.0;   // adaptive stepping: the accepted attempt's norm
     using C = cx<T>;
@@ -353,6 +357,23 @@ struct Engine final : EngineBase {
         check_err_flag();
         if (dtype != PHX_F32 && dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, "bad host dtype");
         if (field == PHX_FFT_MASK_PLUS || field == PHX_FFT_MASK_MINUS) fail(PHX_ERR_UNSUPPORTED, "mask read-back not provided");
+        if (field == PHX_FFT_PLUS || field == PHX_FFT_MINUS) {
+            const int q = field == PHX_FFT_MINUS ? 1 : 0;
+            if (q >= comps) fail(PHX_ERR_INVALID_ARG, "fft_minus needs TE/TM mode");
+            if (!keep_spectrum || !spectrum[q].p) fail(PHX_ERR_INVALID_ARG, "the spectrum is kept after phx_set_spectrum_output(h, 1)");
+            const long long n2 = 2LL * N_r * N_c;
+            if (count != n2) fail(PHX_ERR_INVALID_ARG, "expected " + std::to_string(n2) + " values");
+            std::vector<T> tmp((size_t)n2);
+            PHX_CUDA(cudaMemcpyAsync(tmp.data(), spectrum[q].p, sizeof(T) * (size_t)n2, cudaMemcpyDeviceToHost, stream));
+            PHX_CUDA(cudaStreamSynchronize(stream));
+            for (long long i = 0; i < n2; ++i) {
+                if (dtype == PHX_F64)
+                    static_cast<double*>(host)[i] = (double)tmp[i];
+                else
+                    static_cast<float*>(host)[i] = (float)tmp[i];
+            }
+            return;
+        }
         FieldRef f = field_ref(field, group);
         const long long N = (long long)N_r * N_c;
         const long long want = f.complex ? 2 * N : N;
@@ -389,9 +410,29 @@ struct Engine final : EngineBase {
     // copies in or out; other shapes reinterpret the row-major matrix as N_c
     // rows of N_r, which only a contiguous copy can express.
     bool fft_in_place = false;
+    // phx_set_spectrum_output: the k-space field of the last filter time
+    bool keep_spectrum = false;
+    DevBuf spectrum[2];
+    void set_spectrum_output(bool enable) override {
+        keep_spectrum = enable;
+        if (have_plan) {
+            PHX_CUDA(cudaStreamSynchronize(stream));
+            cufftDestroy(plan);
+            have_plan = false;
+        }
+        if (enable || have_mask[0] || have_mask[1]) ensure_fft();
+        if (enable)
+            for (int q = 0; q < comps; ++q)
+                if (!spectrum[q].p) {
+                    spectrum[q].alloc(sizeof(C) * (size_t)N_r * N_c, stream);
+                    PHX_CUDA(cudaMemsetAsync(spectrum[q].p, 0, sizeof(C) * (size_t)N_r * N_c, stream));
+                }
+    }
     void ensure_fft() {
         if (have_plan) return;
-        fft_in_place = N_r == N_c && !std::getenv("PHX_FFT_CONTIGUOUS");
+        // the spectrum is kept from the contiguous transform, whose plan has the
+        // reference's (N_c, N_r) dimensions
+        fft_in_place = N_r == N_c && !keep_spectrum && !std::getenv("PHX_FFT_CONTIGUOUS");
         if (fft_in_place) {
             int n[2] = {N_r, N_c};
             int embed[2] = {(int)rows, (int)pitch};
@@ -1219,11 +1260,31 @@ struct Engine final : EngineBase {
     // ------------------------------------------------------------ FFT filter
     void fft_filter() {
         for (int q = 0; q < comps; ++q) {
-            if (!have_mask[q]) continue;
+            if (!have_mask[q] && !keep_spectrum) continue;
             const long long N = (long long)N_r * N_c;
             const int blocks = (int)std::min<long long>((N + 255) / 256, 148 * 16);
             cudaEvent_t a = nullptr;
             prof_begin(a);
+            if (keep_spectrum) {
+                // applyFFTFilter with its fft_plus buffer kept: transform, mask / N
+                // where a mask is set, keep, and back only where it was masked
+                ensure_fft();
+                gather_interior_kernel<T><<<blocks, 256, 0, stream>>>(cplane(psi[q]), pitch, N_r, N_c, reinterpret_cast<C*>(fft_x.p));
+                exec_fft(CUFFT_FORWARD);
+                if (have_mask[q])
+                    mask_kernel<T><<<blocks, 256, 0, stream>>>(reinterpret_cast<C*>(fft_x.p), reinterpret_cast<const T*>(mask[q].p), N);
+                PHX_CUDA(cudaMemcpyAsync(spectrum[q].p, fft_x.p, sizeof(C) * (size_t)N, cudaMemcpyDeviceToDevice, stream));
+                launches += have_mask[q] ? 2 : 1;
+                if (have_mask[q]) {
+                    exec_fft(CUFFT_INVERSE);
+                    scatter_interior_kernel<T><<<blocks, 256, 0, stream>>>(reinterpret_cast<C*>(fft_x.p), cplane(psi[q]), pitch, N_r,
+                                                                           N_c, P.periodic_x, P.periodic_y);
+                    ++launches;
+                }
+                prof_end(PHX_KERNEL_FILTER, a, (double)N * (6 * sizeof(C) + sizeof(T)));
+                PHX_CUDA(cudaGetLastError());
+                continue;
+            }
             if (fft_in_place) {
                 // applyFFTFilter on the padded plane itself: FFT, (data / N) * mask,
                 // inverse FFT, then the ring's images / zeros again
@@ -1284,8 +1345,8 @@ struct Engine final : EngineBase {
                 step_rk4();
             } else if (P.iterator == PHX_ITER_SSFM) {
                 step_ssfm();
-            } else if (tab.adaptive && !(imag_time() && !P.adaptive)) {
-                step_adaptive(P.adaptive != 0, acc, rej);
+            } else if (tab.adaptive && !(imag_time() && !adaptive_now())) {
+                step_adaptive(adaptive_now(), acc, rej);
             } else {
                 step_tableau();  // imaginary time: normalised inside
             }
@@ -1296,7 +1357,7 @@ struct Engine final : EngineBase {
                         imag_normalize_device(psi[q], true, kNormBlocks);
                         if (P.use_reservoir) imag_normalize_device(nres[q], false, kNormBlocks);
                     }
-                } else if (tab.adaptive && P.adaptive) {
+                } else if (tab.adaptive && adaptive_now()) {
                     imag_normalize_host(psi[0], imag_nrm);
                 }
             }
@@ -1305,9 +1366,9 @@ struct Engine final : EngineBase {
             ++noise_iteration;
             if (t - fft_cached_t < fft_every) continue;
             fft_cached_t = t;
-            if (have_mask[0] || have_mask[1]) {
+            if (have_mask[0] || have_mask[1] || keep_spectrum) {
                 fft_filter();
-                ++filt;
+                if (have_mask[0] || have_mask[1]) ++filt;
             }
         }
         // RK4 work stays queued on the stream (no host sync); DP45 synchronised
@@ -1815,6 +1876,61 @@ phx_status phx_set_field(phx_handle* h, int32_t field, int32_t group, const void
 phx_status phx_get_field(phx_handle* h, int32_t field, int32_t group, void* host, int64_t count, int32_t host_dtype) {
     if (!h) return PHX_ERR_INVALID_ARG;
     return guard(h, [&] { h->eng->get_field(field, group, host, count, host_dtype); });
+}
+
+phx_status phx_set_temporal_table(phx_handle* h, int32_t envelope, int32_t group, const double* t, const double* re,
+                                  const double* im, int64_t n) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (!t || !re || !im) phx::fail(PHX_ERR_INVALID_ARG, "NULL table");
+        if (n < 2) phx::fail(PHX_ERR_INVALID_ARG, "a temporal table needs at least 2 points");
+        phx::TemporalSpec s;
+        s.kind = PHX_TEMPORAL_LOADED;
+        s.tt.assign(t, t + n);
+        s.re.assign(re, re + n);
+        s.im.assign(im, im + n);
+        for (int64_t i = 0; i < n; ++i) {
+            if (!std::isfinite(t[i]) || !std::isfinite(re[i]) || !std::isfinite(im[i]))
+                phx::fail(PHX_ERR_INVALID_ARG, "temporal table values must be finite");
+            if (i > 0 && !(t[i] >= t[i - 1])) phx::fail(PHX_ERR_INVALID_ARG, "temporal table times must ascend");
+        }
+        auto& P = h->eng->P;
+        if (envelope == PHX_ENV_PUMP) {
+            if (group < 0 || group >= P.n_pump_groups) phx::fail(PHX_ERR_INVALID_ARG, "pump group out of range");
+            for (int64_t i = 0; i < n; ++i)
+                if (im[i] != 0.0) phx::fail(PHX_ERR_UNSUPPORTED, "complex pump tables make the reservoir complex");
+            h->eng->pump_t[group] = s;
+        } else if (envelope == PHX_ENV_POTENTIAL) {
+            if (group < 0 || group >= P.n_potential_groups) phx::fail(PHX_ERR_INVALID_ARG, "potential group out of range");
+            h->eng->pot_t[group] = s;
+        } else if (envelope == PHX_ENV_PULSE) {
+            if (group < 0 || group >= P.n_pulse_groups) phx::fail(PHX_ERR_INVALID_ARG, "pulse group out of range");
+            h->eng->pulse_t[group] = s;
+        } else {
+            phx::fail(PHX_ERR_INVALID_ARG, "unknown envelope family");
+        }
+    });
+}
+
+phx_status phx_iterate(phx_handle* h, int32_t force_fixed_time_step, phx_step_info* info) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        cudaSetDevice(h->eng->P.device);
+        struct Reset {
+            phx::EngineBase* e;
+            ~Reset() { e->force_fixed = false; }
+        } reset{h->eng.get()};
+        h->eng->force_fixed = force_fixed_time_step != 0;
+        h->eng->step(1, info);
+    });
+}
+
+phx_status phx_set_spectrum_output(phx_handle* h, int32_t enable) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        cudaSetDevice(h->eng->P.device);
+        h->eng->set_spectrum_output(enable != 0);
+    });
 }
 
 phx_status phx_set_temporal(phx_handle* h, int32_t envelope, int32_t group, int32_t kind, double t0, double sigma, double freq) {
