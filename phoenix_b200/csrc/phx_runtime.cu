@@ -20,6 +20,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "../../include/phx.h"
@@ -118,7 +119,7 @@ struct Engine final : EngineBase {
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 5];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 7];
     static constexpr int kRingBlocks = 64;
     static constexpr int kNormBlocks = 296;
     // imaginary-time propagation (--imagTime): k-stack sums with the complex
@@ -234,7 +235,7 @@ struct Engine final : EngineBase {
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
     static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
-    static constexpr int kFusedShapes = 5;  // shape 8: persistent TMA-fed variant
+    static constexpr int kFusedShapes = 7;  // shapes 8-10: persistent TMA-fed variants
     int n_candidates() const { return fused_eligible_static() ? kShapes + kFusedShapes : kShapes; }
     bool is_fused(int sh) const { return sh >= kFusedShape; }
     int cur_shape() const { return shape >= 0 ? shape : tune_step % n_candidates(); }
@@ -643,24 +644,29 @@ struct Engine final : EngineBase {
         rk4_fused_kernel<T, RES, TW, TH, NT><<<grid, NT, 0, stream>>>(F);
     }
     // ---- TMA-fed persistent variant
-    int tma_blocks_per_sm = 0, sm_count = 0;
+    int sm_count = 0;
+    std::map<const void*, int> tma_blocks;  // CTAs per SM of each TMA kernel variant
     void tensor_map(CUtensorMap* m, void* alloc_base, bool complex, int box_w_points, int box_h) {
         plane_tensor_map<T>(m, alloc_base, complex, pitch, rows, box_w_points, box_h);
     }
+    // tensor maps depend on the planes and on the tile shape (box size): a
+    // map encoded for another shape would expect another byte count
     struct MapPair {
         const void* psi = nullptr;
         const void* n = nullptr;
+        int tw = 0, th = 0;
         CUtensorMap psi_map, n_map;
     };
     MapPair tma_maps[2];
     int tma_next = 0;
     CUtensorMap tma_pump_map, tma_pot_map;
-    bool tma_inputs_ready = false;
-    template <bool RES, int TW, int TH, int NT>
+    int tma_inputs_tw = 0, tma_inputs_th = 0;
+    template <bool RES, int TW, int TH, int NT, int MINB = 1>
     void go_tma(const FusedParams<T>& F) {
         using Lay = TmaLayout<T, TW, TH>;
         static_assert(TW % 4 == 0, "TMA box x alignment needs tile origins on 16-byte boundaries");
-        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT>;
+        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT, MINB>;
+        int& tma_blocks_per_sm = tma_blocks[reinterpret_cast<const void*>(kern)];
         if (!tma_blocks_per_sm) {
             PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
             PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_blocks_per_sm, kern, NT, Lay::total));
@@ -675,7 +681,7 @@ struct Engine final : EngineBase {
         // the state alternates between two planes, so two encodings are kept
         MapPair* mp = nullptr;
         for (auto& m : tma_maps)
-            if (m.psi == psi[0].p && m.n == nres[0].p) mp = &m;
+            if (m.psi == psi[0].p && m.n == nres[0].p && m.tw == TW && m.th == TH) mp = &m;
         if (!mp) {
             mp = &tma_maps[tma_next];
             tma_next ^= 1;
@@ -685,11 +691,14 @@ struct Engine final : EngineBase {
                        TH + 6);
             mp->psi = psi[0].p;
             mp->n = nres[0].p;
+            mp->tw = TW;
+            mp->th = TH;
         }
-        if (!tma_inputs_ready) {
+        if (tma_inputs_tw != TW || tma_inputs_th != TH) {
             tensor_map(&tma_pump_map, pump[0].p, false, TW + 8, TH + 6);
             tensor_map(&tma_pot_map, pot[0].p, false, TW + 8, TH + 6);
-            tma_inputs_ready = true;
+            tma_inputs_tw = TW;
+            tma_inputs_th = TH;
         }
         Q.psi_map = mp->psi_map;
         Q.n_map = mp->n_map;
@@ -716,9 +725,12 @@ struct Engine final : EngineBase {
     template <bool RES>
     void go_fused(const FusedParams<T>& F) {
         constexpr bool f32 = sizeof(T) == 4;
-        if (cur_shape() - kFusedShape == 4) {
-            go_tma<RES, 32, f32 ? 32 : 16, 256>(F);
-            return;
+        switch (cur_shape() - kFusedShape) {
+            case 4: go_tma<RES, 32, f32 ? 32 : 16, 256>(F); return;
+            // 12 warps per CTA, two CTAs per SM: registers capped at 85
+            case 5: go_tma<RES, 32, f32 ? 32 : 16, 384, 2>(F); return;
+            case 6: go_tma<RES, 64, f32 ? 16 : 8, 384, 2>(F); return;
+            default: break;
         }
         switch (cur_shape() - kFusedShape) {
             case 0: go_fused_shape<RES, 32, f32 ? 32 : 16, 256>(F); break;

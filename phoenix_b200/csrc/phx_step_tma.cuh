@@ -317,8 +317,9 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
     }
 }
 
-template <typename T, bool RES, int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) rk4_tma_kernel(const __grid_constant__ TmaParams<T> Q) {
+// MINB: CTAs per SM the register allocation must leave room for
+template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) rk4_tma_kernel(const __grid_constant__ TmaParams<T> Q) {
     auto tile_of = [&](int g) {
         TileRef<T> R;
         R.psi_map = &Q.psi_map;

@@ -143,7 +143,7 @@ SHAPE_CASES = ["rk4_f64_zero", "rk4_f64_periodic", "rk4_f64_mixed_rect", "rk4_f3
                "rk4_f64_temporal", "rk4_f64_nores"]
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("name", SHAPE_CASES)
 def test_every_launch_shape_gives_identical_results(require_gpu, shape, name, monkeypatch):
     """The autotuner may pick any launch shape (0-3: one kernel per RK stage,
@@ -174,7 +174,7 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
     n = 1024
     wl = B.workload(n)
     res = {}
-    for shape in (2, 4, 5, 6, 7, 8):
+    for shape in (2, 4, 5, 6, 7, 8, 9, 10):
         monkeypatch.setenv("PHX_STAGE_SHAPE", str(shape))
         sp = B.system(pb, n, "f32", 0)
         sp.fft_every = 1e12
@@ -186,9 +186,38 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
             info = s.run(25)
             assert info.launch_shape == shape
             res[shape] = (s.get_field("psi_plus"), s.get_field("n_plus"))
-    for shape in (4, 5, 6, 7, 8):
+    for shape in (4, 5, 6, 7, 8, 9, 10):
         np.testing.assert_array_equal(res[2][0], res[shape][0])
         np.testing.assert_array_equal(res[2][1], res[shape][1])
+
+
+def test_autotuning_across_every_shape_is_bit_identical(require_gpu, monkeypatch):
+    """The first iterations of a handle cycle through every launch shape (TMA
+    tile shapes of different sizes among them, whose tensor maps differ): the
+    result equals a run on one fixed shape."""
+    import bench as B
+
+    n = 256
+    wl = B.workload(n)
+    outs = []
+    for shape in (None, "2"):
+        if shape is None:
+            monkeypatch.delenv("PHX_STAGE_SHAPE", raising=False)
+        else:
+            monkeypatch.setenv("PHX_STAGE_SHAPE", shape)
+        sp = B.system(pb, n, "f32", 0)
+        sp.fft_every = 1e12
+        with pb.Solver(sp) as s:
+            s.set_field("psi_plus", wl["psi0"])
+            s.set_field("n_plus", np.zeros((n, n)))
+            s.set_field("pump_plus", wl["pump"], 0)
+            s.set_field("potential_plus", wl["potential"], 0)
+            info = s.run(40)
+            if shape is None:
+                assert info.launch_shape >= 0  # tuning finished within the run
+            outs.append((s.get_field("psi_plus"), s.get_field("n_plus")))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
 
 
 def test_bad_field_shape_is_rejected(require_gpu):
