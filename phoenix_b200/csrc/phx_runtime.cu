@@ -30,6 +30,7 @@
 #include "phx_stage_tetm.cuh"
 #include "phx_step_fused.cuh"
 #include "phx_step_tma.cuh"
+#include "phx_step_tetm_fused.cuh"
 #include "phx_rt.hpp"
 #include "phx_adjoint.cuh"
 #include "phx_ssfm.cuh"
@@ -594,6 +595,26 @@ struct Engine final : EngineBase {
     void go_tetm(const TetmParams<T>& Q, dim3 grid) {
         stage_tetm_kernel<T, KIND, kShapeRB[SH], kShapeWarps[SH]><<<grid, 32 * kShapeWarps[SH], 0, stream>>>(Q);
     }
+    // TE/TM parameters of one stage: S wired for the plus component, the
+    // minus component's planes from wire(., 1)
+    template <typename Wire>
+    TetmParams<T> tetm_params(const StageParams<T>& S, Wire wire) {
+        TetmParams<T> Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.p = S;
+        StageParams<T> M = S;
+        wire(M, 1);
+        Q.psi_in = M.psi_in, Q.n_in = M.n_in, Q.psi0 = M.psi0, Q.n0 = M.n0, Q.psi_out = M.psi_out;
+        Q.n_out = M.n_out, Q.acc_psi = M.acc_psi, Q.acc_n = M.acc_n, Q.k_psi = M.k_psi, Q.k_n = M.k_n;
+        Q.pump = M.pump, Q.pot = M.pot, Q.pulse = M.pulse;
+        Q.ohb_meff = d.ohb * d.meff;
+        Q.ohb_gpm = d.ohb * (T)P.g_pm;
+        Q.ohb_dlt = d.ohb * (T)P.delta_LT;
+        Q.hidd.re = (T)0.0 / d.dx / d.dy;
+        Q.hidd.im = (T)0.5 / d.dx / d.dy;
+        return Q;
+    }
+
     // Launch stage KIND.  `wire(S, q)` points S at component q's planes; in
     // TE/TM mode the minus component's planes are wired the same way and
     // both polarisations run in one kernel.
@@ -601,19 +622,7 @@ struct Engine final : EngineBase {
     void launch(StageParams<T>& S, Wire wire) {
         wire(S, 0);
         if (P.tetm) {
-            TetmParams<T> Q;
-            std::memset(&Q, 0, sizeof(Q));
-            Q.p = S;
-            StageParams<T> M = S;
-            wire(M, 1);
-            Q.psi_in = M.psi_in, Q.n_in = M.n_in, Q.psi0 = M.psi0, Q.n0 = M.n0, Q.psi_out = M.psi_out;
-            Q.n_out = M.n_out, Q.acc_psi = M.acc_psi, Q.acc_n = M.acc_n, Q.k_psi = M.k_psi, Q.k_n = M.k_n;
-            Q.pump = M.pump, Q.pot = M.pot, Q.pulse = M.pulse;
-            Q.ohb_meff = d.ohb * d.meff;
-            Q.ohb_gpm = d.ohb * (T)P.g_pm;
-            Q.ohb_dlt = d.ohb * (T)P.delta_LT;
-            Q.hidd.re = (T)0.0 / d.dx / d.dy;
-            Q.hidd.im = (T)0.5 / d.dx / d.dy;
+            TetmParams<T> Q = tetm_params(S, wire);
             dim3 grid((unsigned)grid_x(S.c0, S.c1), (unsigned)grid_y(S.r0, S.r1));
             cudaEvent_t a = nullptr;
             prof_begin(a);
@@ -788,7 +797,72 @@ struct Engine final : EngineBase {
         return true;
     }
 
+    // ---- TE/TM: the whole iteration in one kernel (phx_step_tetm_fused.cuh);
+    // PHX_TETM_FUSED=1 selects it, PHX_TETM_FUSED=0 the four stage kernels
+    bool tetm_fused_set = false;
+    static bool tetm_fused_on() {
+        const char* e = std::getenv("PHX_TETM_FUSED");
+        return e && e[0] == '1';
+    }
+    template <int TW, int TH, int NT>
+    void go_tetm_fused(const TetmFusedParams<T>& F) {
+        using Lay = TetmFusedLayout<T, TW, TH>;
+        auto kern = rk4_tetm_fused_kernel<T, TW, TH, NT>;
+        if (!tetm_fused_set) {
+            PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::bytes));
+            tetm_fused_set = true;
+        }
+        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+        kern<<<grid, NT, Lay::bytes, stream>>>(F);
+    }
+    void step_rk4_tetm_fused() {
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
+        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
+        TetmFusedParams<T> F;
+        std::memset(&F, 0, sizeof(F));
+        for (int s = 1; s <= 4; ++s) {
+            // the per-stage kernels' parameters of stage s (step_rk4 below)
+            StageParams<T> S = base_params(0);
+            set_coefficients(S, cw[s - 1]);
+            S.stage = s;
+            S.b = bw[s - 1];
+            if (s < 4) S.dtw = dt * aw[s - 1];
+            S.w_sum = s < 4 ? aw[s - 1] : right_fold(bw, 4);
+            auto wire = [this](StageParams<T>& X, int q) {
+                X.pump = rplane(pump[q]);
+                X.pot = rplane(pot[q]);
+                X.pulse = cplane(pulse[q]);
+            };
+            wire(S, 0);
+            F.st[s - 1] = tetm_params(S, wire);
+        }
+        for (int q = 0; q < 2; ++q) {
+            F.psi0[q] = cplane(psi[q]);
+            F.n0[q] = rplane(nres[q]);
+            F.psi1[q] = cplane(sbuf_psi[q][0]);
+            F.n1[q] = rplane(sbuf_n[q][0]);
+        }
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        if constexpr (sizeof(T) == 4)
+            go_tetm_fused<32, 16, 256>(F);
+        else
+            go_tetm_fused<32, 8, 128>(F);
+        // read psi, n (both components) + pump, potential per group; write psi, n
+        const double pt = 2.0 * (2.0 * sizeof(C) + 2.0 * sizeof(T)) +
+                          2.0 * sizeof(T) * (P.n_pump_groups + P.n_potential_groups) + 2.0 * sizeof(C) * P.n_pulse_groups;
+        prof_end(PHX_KERNEL_RK4_FUSED, a, pt * (double)N_r * N_c);
+        ++launches;
+        PHX_CUDA(cudaGetLastError());
+        swap_state_with(0);
+    }
+
     void step_rk4() {
+        if (P.tetm && tetm_fused_on()) {
+            step_rk4_tetm_fused();
+            return;
+        }
         if (is_fused(cur_shape()) && step_rk4_fused()) return;
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
         const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
