@@ -798,11 +798,11 @@ struct Engine final : EngineBase {
     }
 
     // ---- TE/TM: the whole iteration in one kernel (phx_step_tetm_fused.cuh);
-    // PHX_TETM_FUSED=1 selects it, PHX_TETM_FUSED=0 the four stage kernels
+    // PHX_TETM_FUSED=0 selects the four stage kernels instead
     bool tetm_fused_set = false;
     static bool tetm_fused_on() {
         const char* e = std::getenv("PHX_TETM_FUSED");
-        return e && e[0] == '1';
+        return !(e && e[0] == '0');
     }
     template <int TW, int TH, int NT>
     void go_tetm_fused(const TetmFusedParams<T>& F) {
@@ -846,9 +846,9 @@ struct Engine final : EngineBase {
         cudaEvent_t a = nullptr;
         prof_begin(a);
         if constexpr (sizeof(T) == 4)
-            go_tetm_fused<32, 16, 256>(F);
+            go_tetm_fused<32, 16, 512>(F);
         else
-            go_tetm_fused<32, 8, 128>(F);
+            go_tetm_fused<32, 8, 512>(F);
         // read psi, n (both components) + pump, potential per group; write psi, n
         const double pt = 2.0 * (2.0 * sizeof(C) + 2.0 * sizeof(T)) +
                           2.0 * sizeof(T) * (P.n_pump_groups + P.n_potential_groups) + 2.0 * sizeof(C) * P.n_pulse_groups;
@@ -858,9 +858,73 @@ struct Engine final : EngineBase {
         swap_state_with(0);
     }
 
+    // ---- scalar RK4 with what rk4_tma_kernel does not take (noise, pulses,
+    // several groups): one kernel per iteration as well; PHX_GENERAL_FUSED=0
+    // selects the four stage kernels
+    bool general_set = false;
+    static bool general_fused_on() {
+        const char* e = std::getenv("PHX_GENERAL_FUSED");
+        return !(e && e[0] == '0');
+    }
+    template <bool RES, int TW, int TH, int NT>
+    void go_general(const ScalarFusedParams<T>& F) {
+        using Lay = ScalarFusedLayout<T, TW, TH>;
+        auto kern = rk4_scalar_general_kernel<T, RES, TW, TH, NT>;
+        if (!general_set) {
+            PHX_CUDA(cudaFuncSetAttribute(rk4_scalar_general_kernel<T, true, TW, TH, NT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::bytes));
+            PHX_CUDA(cudaFuncSetAttribute(rk4_scalar_general_kernel<T, false, TW, TH, NT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::bytes));
+            general_set = true;
+        }
+        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+        kern<<<grid, NT, Lay::bytes, stream>>>(F);
+    }
+    void step_rk4_general() {
+        const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
+        const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
+        const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
+        ScalarFusedParams<T> F;
+        std::memset(&F, 0, sizeof(F));
+        for (int s = 1; s <= 4; ++s) {
+            // the per-stage kernels' parameters of stage s (step_rk4 below)
+            StageParams<T> S = base_params(0);
+            set_coefficients(S, cw[s - 1]);
+            S.stage = s;
+            S.b = bw[s - 1];
+            if (s < 4) S.dtw = dt * aw[s - 1];
+            S.w_sum = s < 4 ? aw[s - 1] : right_fold(bw, 4);
+            S.pump = rplane(pump[0]);
+            S.pot = rplane(pot[0]);
+            S.pulse = cplane(pulse[0]);
+            F.st[s - 1] = S;
+        }
+        F.psi0 = cplane(psi[0]);
+        F.n0 = rplane(nres[0]);
+        F.psi1 = cplane(sbuf_psi[0][0]);
+        F.n1 = rplane(sbuf_n[0][0]);
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        constexpr bool f32 = sizeof(T) == 4;
+        if (P.use_reservoir)
+            go_general<true, 32, f32 ? 16 : 8, 512>(F);
+        else
+            go_general<false, 32, f32 ? 16 : 8, 512>(F);
+        const double pt = 2.0 * (sizeof(C) + (P.use_reservoir ? sizeof(T) : 0.0)) +
+                          sizeof(T) * (P.n_pump_groups + P.n_potential_groups) + sizeof(C) * P.n_pulse_groups;
+        prof_end(PHX_KERNEL_RK4_FUSED, a, pt * (double)N_r * N_c);
+        ++launches;
+        PHX_CUDA(cudaGetLastError());
+        swap_state_with(0);
+    }
+
     void step_rk4() {
         if (P.tetm && tetm_fused_on()) {
             step_rk4_tetm_fused();
+            return;
+        }
+        if (!P.tetm && !fused_eligible_static() && general_fused_on()) {
+            step_rk4_general();
             return;
         }
         if (is_fused(cur_shape()) && step_rk4_fused()) return;

@@ -1,6 +1,7 @@
-"""The one-kernel TE/TM RK4 iteration (rk4_tetm_fused_kernel) against the
-per-stage TE/TM kernels (PHX_TETM_FUSED=0), which the reference fixtures pin
-(tests/test_gpu_parity.py, tetm_*): bit-identical fields on grids that are not
+"""The one-kernel RK4 iterations of the TE/TM spinor (rk4_tetm_fused_kernel) and
+of the scalar model beyond the TMA iteration (rk4_scalar_general_kernel), the defaults,
+against the per-stage kernels (PHX_TETM_FUSED=0, PHX_GENERAL_FUSED=0), which the
+reference fixtures also pin (tests/test_gpu_parity.py): bit-identical fields on grids that are not
 multiples of the tile, for both boundary kinds, several pump / potential /
 pulse groups with time dependence, and stochastic noise."""
 import numpy as np
@@ -49,5 +50,43 @@ def test_fused_tetm_iteration_matches_stage_kernels(require_gpu, monkeypatch, dt
     assert info.iterations == 12
     monkeypatch.setenv("PHX_TETM_FUSED", "0")
     staged, _ = run(case, fields, 12)
+    for k in fused:
+        np.testing.assert_array_equal(fused[k], staged[k], err_msg=k)
+
+
+def make_scalar(n_c, n_r, dtype, px, py, dw, reservoir):
+    case, f = make(n_c, n_r, dtype, px, py, dw)
+    case.pop("tetm")
+    case["potential_t"] = [("iexp", 0.02, 0.1, 4.0), None]  # a complex potential coefficient
+    if not reservoir:
+        case["pumps"], case["pump_t"] = [], []
+        f.pop("n_plus")
+    return case, f
+
+
+def run_scalar(case, fields, iters):
+    sp = pb.system_from_case(case)
+    with pb.Solver(sp) as s:
+        pb.load_case_fields(s, case, fields)
+        info = s.run(iters)
+        out = {"psi_plus": s.get_field("psi_plus")}
+        if sp.use_reservoir:
+            out["n_plus"] = s.get_field("n_plus")
+        return out, info
+
+
+@pytest.mark.parametrize("dtype,px,py,dw,res", [("f32", 1, 1, 0.02, True), ("f32", 0, 1, 0.0, False),
+                                                ("f64", 1, 0, 0.02, True), ("f64", 0, 0, 0.02, False)])
+def test_general_scalar_iteration_matches_stage_kernels(require_gpu, monkeypatch, dtype, px, py, dw, res):
+    """Scalar runs the TMA iteration does not take (noise, pulses, two pump and
+    potential groups, a complex temporal coefficient) run one kernel per
+    iteration (rk4_scalar_general_kernel): the same bits as the stage kernels."""
+    case, fields = make_scalar(70, 46, dtype, px, py, dw, res)
+    monkeypatch.setenv("PHX_GENERAL_FUSED", "1")
+    fused, info = run_scalar(case, fields, 12)
+    assert info.iterations == 12 and info.kernel_launches <= 12 * 3
+    monkeypatch.setenv("PHX_GENERAL_FUSED", "0")
+    staged, info2 = run_scalar(case, fields, 12)
+    assert info2.kernel_launches >= 12 * 4
     for k in fused:
         np.testing.assert_array_equal(fused[k], staged[k], err_msg=k)
