@@ -69,12 +69,13 @@ __device__ __forceinline__ void neighbours(const Row<T>& r, int lane, cx<T>* L, 
     }
 }
 
-// Both polarisations at one point: k of psi+, n+, psi-, n-.
-template <typename T>
-__device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, cx<T> wp, cx<T> upp, cx<T> dnp, cx<T> lp, cx<T> rp,
-                                         cx<T> ulp, cx<T> urp, cx<T> dlp, cx<T> drp, cx<T> wm, cx<T> upm, cx<T> dnm, cx<T> lm,
-                                         cx<T> rm, cx<T> ulm, cx<T> urm, cx<T> dlm, cx<T> drm, T rvp, T rvm, cx<T>& kwp, T& krp,
-                                         cx<T>& kwm, T& krm) {
+// Both polarisations at one point: k of psi+, n+, psi-, n-; the pointwise
+// inputs come from `src` (TetmGlobalSrc or a shared-memory copy)
+template <typename T, typename Src>
+__device__ __forceinline__ void rhs_tetm_src(const TetmParams<T>& Q, const Src& src, cx<T> wp, cx<T> upp, cx<T> dnp, cx<T> lp,
+                                             cx<T> rp, cx<T> ulp, cx<T> urp, cx<T> dlp, cx<T> drp, cx<T> wm, cx<T> upm,
+                                             cx<T> dnm, cx<T> lm, cx<T> rm, cx<T> ulm, cx<T> urm, cx<T> dlm, cx<T> drm, T rvp,
+                                             T rvm, cx<T>& kwp, T& krp, cx<T>& kwm, T& krm) {
     const StageParams<T>& P = Q.p;
     const cx<T> in_wf_plus_mi = mk(wp.im, rmul((T)-1.0, wp.re));
     const cx<T> in_wf_minus_mi = mk(wm.im, rmul((T)-1.0, wm.re));
@@ -99,7 +100,7 @@ __device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, 
     // wavefunction plus
     cx<T> res = smul(Q.ohb_meff, hrp);
     for (int g = 0; g < P.n_pot; ++g) {
-        const cx<T> pot = smul(__ldg(P.pot + idx + g * P.plane), P.pot_c[g]);
+        const cx<T> pot = smul(src.pot(0, g), P.pot_c[g]);
         res = cadd(res, cmul(smul(P.ohb, pot), in_wf_plus_mi));
     }
     res = cadd(res, smul(rmul(P.ohb_gc, npl), in_wf_plus_mi));
@@ -108,18 +109,18 @@ __device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, 
     res = csub(res, smul(P.half_gamma_c, wp));
     res = cadd(res, smul(rmul(Q.ohb_gpm, nmi), in_wf_plus_mi));
     res = cadd(res, smul(Q.ohb_dlt, hcp));
-    for (int g = 0; g < P.n_pulse; ++g) res = cadd(res, cmul(smul(P.ohb, ld1(P.pulse + idx + g * P.plane)), P.pulse_c[g]));
+    for (int g = 0; g < P.n_pulse; ++g) res = cadd(res, cmul(smul(P.ohb, src.pulse(0, g)), P.pulse_c[g]));
     if (P.noise.on) res = csub(res, noise_drift(P, in_wf_plus_mi));
     kwp = res;
     // reservoir plus
     T r = rmul(-radd(P.gamma_r, rmul(P.R, npl)), rvp);
-    for (int g = 0; g < P.n_pump; ++g) r = radd(r, rmul(__ldg(P.pump + idx + g * P.plane), P.pump_c[g].re));
+    for (int g = 0; g < P.n_pump; ++g) r = radd(r, rmul(src.pump(0, g), P.pump_c[g].re));
     if (P.noise.on) r = radd(r, rdiv(rmul(P.R, rvp), P.dV));
     krp = r;
     // wavefunction minus
     res = smul(Q.ohb_meff, hrm);
     for (int g = 0; g < P.n_pot; ++g) {
-        const cx<T> pot = smul(__ldg(Q.pot + idx + g * P.plane), P.pot_c[g]);
+        const cx<T> pot = smul(src.pot(1, g), P.pot_c[g]);
         res = cadd(res, cmul(smul(P.ohb, pot), in_wf_minus_mi));
     }
     res = cadd(res, smul(rmul(P.ohb_gc, nmi), in_wf_minus_mi));
@@ -128,14 +129,35 @@ __device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, 
     res = csub(res, smul(P.half_gamma_c, wm));
     res = cadd(res, smul(rmul(Q.ohb_gpm, npl), in_wf_minus_mi));
     res = cadd(res, smul(Q.ohb_dlt, hcm));
-    for (int g = 0; g < P.n_pulse; ++g) res = cadd(res, cmul(smul(P.ohb, ld1(Q.pulse + idx + g * P.plane)), P.pulse_c[g]));
+    for (int g = 0; g < P.n_pulse; ++g) res = cadd(res, cmul(smul(P.ohb, src.pulse(1, g)), P.pulse_c[g]));
     if (P.noise.on) res = csub(res, noise_drift(P, in_wf_minus_mi));
     kwm = res;
     // reservoir minus
     r = rmul(-radd(P.gamma_r, rmul(P.R, nmi)), rvm);
-    for (int g = 0; g < P.n_pump; ++g) r = radd(r, rmul(__ldg(Q.pump + idx + g * P.plane), P.pump_c[g].re));
+    for (int g = 0; g < P.n_pump; ++g) r = radd(r, rmul(src.pump(1, g), P.pump_c[g].re));
     if (P.noise.on) r = radd(r, rdiv(rmul(P.R, rvm), P.dV));
     krm = r;
+}
+
+// The pointwise inputs of one point (pump, potential, pulse of group g of
+// component c) read from the global planes
+template <typename T>
+struct TetmGlobalSrc {
+    const TetmParams<T>& Q;
+    long long idx;
+    __device__ __forceinline__ T pump(int c, int g) const { return __ldg((c ? Q.pump : Q.p.pump) + idx + g * Q.p.plane); }
+    __device__ __forceinline__ T pot(int c, int g) const { return __ldg((c ? Q.pot : Q.p.pot) + idx + g * Q.p.plane); }
+    __device__ __forceinline__ cx<T> pulse(int c, int g) const { return ld1((c ? Q.pulse : Q.p.pulse) + idx + g * Q.p.plane); }
+};
+
+// Both polarisations at one point, the pointwise inputs from the global planes
+template <typename T>
+__device__ __forceinline__ void rhs_tetm(const TetmParams<T>& Q, long long idx, cx<T> wp, cx<T> upp, cx<T> dnp, cx<T> lp, cx<T> rp,
+                                         cx<T> ulp, cx<T> urp, cx<T> dlp, cx<T> drp, cx<T> wm, cx<T> upm, cx<T> dnm, cx<T> lm,
+                                         cx<T> rm, cx<T> ulm, cx<T> urm, cx<T> dlm, cx<T> drm, T rvp, T rvm, cx<T>& kwp, T& krp,
+                                         cx<T>& kwm, T& krm) {
+    rhs_tetm_src<T>(Q, TetmGlobalSrc<T>{Q, idx}, wp, upp, dnp, lp, rp, ulp, urp, dlp, drp, wm, upm, dnm, lm, rm, ulm, urm, dlm,
+                    drm, rvp, rvm, kwp, krp, kwm, krm);
 }
 
 template <typename T, int KIND, int RB, int WARPS>

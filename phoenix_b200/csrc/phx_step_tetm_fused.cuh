@@ -45,7 +45,26 @@ struct TetmFusedLayout {
     static constexpr int acc_off = psi_bytes;
     static constexpr int xi_off = acc_off + 2 * NR * (int)sizeof(cx<T>);
     static constexpr int n_off = xi_off + NR * (int)sizeof(cx<T>);
-    static constexpr int bytes = n_off + 6 * NR * (int)sizeof(T);
+    // group 0 of the pump and of the potential, both components
+    static constexpr int in_off = n_off + 6 * NR * (int)sizeof(T);
+    static constexpr int bytes = in_off + 4 * NR * (int)sizeof(T);
+};
+
+// Pointwise inputs of a tile + 3 point: group 0 of the pump and potential
+// from the CTA's shared copy, other groups and pulses from the global planes
+template <typename T>
+struct TetmTileSrc {
+    const TetmParams<T>& Q;
+    long long idx;
+    const T* in;  // [pump+, pump-, pot+, pot-][NR] at this point: in + q
+    int NR;
+    __device__ __forceinline__ T pump(int c, int g) const {
+        return g == 0 ? in[c * NR] : __ldg((c ? Q.pump : Q.p.pump) + idx + g * Q.p.plane);
+    }
+    __device__ __forceinline__ T pot(int c, int g) const {
+        return g == 0 ? in[(2 + c) * NR] : __ldg((c ? Q.pot : Q.p.pot) + idx + g * Q.p.plane);
+    }
+    __device__ __forceinline__ cx<T> pulse(int c, int g) const { return ld1((c ? Q.pulse : Q.p.pulse) + idx + g * Q.p.plane); }
 };
 
 template <typename T, int TW, int TH, int NT>
@@ -57,6 +76,7 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
     cx<T>* acc = reinterpret_cast<cx<T>*>(tetm_smem + Lay::acc_off);  // [2][NR]
     cx<T>* xis = reinterpret_cast<cx<T>*>(tetm_smem + Lay::xi_off);   // [NR]
     T* nv = reinterpret_cast<T*>(tetm_smem + Lay::n_off);             // [6][NR]: n0+, n0-, ns+, ns-, an+, an-
+    T* tin = reinterpret_cast<T*>(tetm_smem + Lay::in_off);           // [4][NR]: pump+, pump-, pot+, pot- (group 0)
     // psi buffer b (0 = A = y0, 1 = B, 2 = C) of component q
     auto pbuf = [&](int b, int q) { return psi + (2 * b + q) * Lay::plane; };
 
@@ -81,6 +101,8 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
         const T a = __ldg(F.n0[0] + g), b = __ldg(F.n0[1] + g);
         nv[i] = a, nv[NR + i] = b, nv[2 * NR + i] = a, nv[3 * NR + i] = b;
         if (P0.noise.on) xis[i] = stage_xi(P0, ty0 - 3 + qy, tx0 - 3 + qx);
+        if (P0.n_pump > 0) tin[i] = __ldg(P0.pump + g), tin[NR + i] = __ldg(F.st[0].pump + g);
+        if (P0.n_pot > 0) tin[2 * NR + i] = __ldg(P0.pot + g), tin[3 * NR + i] = __ldg(F.st[0].pot + g);
     }
     __syncthreads();
 
@@ -106,10 +128,10 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
             const long long idx = (long long)min(gy, rmax) * pitch + min(gx, cmax);
             cx<T> kwp, kwm;
             T krp, krm;
-            rhs_tetm<T>(Q, idx, ip[e], ip[e - SW], ip[e + SW], ip[e - 1], ip[e + 1], ip[e - SW - 1], ip[e - SW + 1],
-                        ip[e + SW - 1], ip[e + SW + 1], im[e], im[e - SW], im[e + SW], im[e - 1], im[e + 1],
-                        im[e - SW - 1], im[e - SW + 1], im[e + SW - 1], im[e + SW + 1], nv[2 * NR + q], nv[3 * NR + q],
-                        kwp, krp, kwm, krm);
+            rhs_tetm_src<T>(Q, TetmTileSrc<T>{Q, idx, tin + q, NR}, ip[e], ip[e - SW], ip[e + SW], ip[e - 1], ip[e + 1],
+                            ip[e - SW - 1], ip[e - SW + 1], ip[e + SW - 1], ip[e + SW + 1], im[e], im[e - SW], im[e + SW],
+                            im[e - 1], im[e + 1], im[e - SW - 1], im[e - SW + 1], im[e + SW - 1], im[e + SW + 1],
+                            nv[2 * NR + q], nv[3 * NR + q], kwp, krp, kwm, krm);
             const cx<T> y0p = pbuf(0, 0)[e], y0m = pbuf(0, 1)[e];
             const T n0p = nv[q], n0m = nv[NR + q];
             // the kRk4First / kRk4Mid / kRk4Last sums of stage_tetm_kernel
