@@ -413,6 +413,36 @@ def _device_us(torch, solver, device, iters):
     return a.elapsed_time(b) * 1e3 / max(info.iterations, 1), info
 
 
+def run_tetm(pb, torch, dev, n):
+    """Config 3 at n x n: TE/TM FP32 RK4, ring pump (radius 20 um, width 3 um) at 1.5x threshold on both
+    polarisations, delta_LT 0.05 meV, g_pm = -0.2 g_c, dt 0.0015 ps at 4096^2 (scaled with dx^2),
+    with noise (dw 1e-3) and without."""
+    out = {}
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n, dtype=np.float64)
+    X, Y = np.meshgrid(x, x)
+    ring = (1.5 * P_TH * np.exp(-(np.sqrt(X ** 2 + Y ** 2) - 20.0) ** 2 / (2 * 3.0 ** 2))).astype(np.float32)
+    del X, Y
+    rng = np.random.default_rng(4)
+    dt = 0.0015 * (4096.0 / n) ** 2
+    for dw in (1e-3, 0.0):
+        sp = pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                                 periodic_boundary_y=True, dtype="f32", iterator="RK4", dt=dt, t0=0.0, t_max=1e12,
+                                 fft_every=1e12, pump_temporal=[pb.Temporal()], device=dev, use_twin_mode=True,
+                                 stochastic_amplitude=dw, random_seed=4)
+        sp.g_pm, sp.delta_LT = -0.2 * PHYS["g_c"], 0.05
+        with pb.Solver(sp) as s:
+            for comp in ("plus", "minus"):
+                psi0 = (1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
+                s.set_field(f"psi_{comp}", psi0)
+                s.set_field(f"pump_{comp}", ring, 0)
+            s.run(12)
+            us, info = _device_us(torch, s, dev, 20)
+            key = f"tetm_{n}_f32_noise" if dw else f"tetm_{n}_f32_deterministic"
+            out[key] = {"us_per_iteration": us, "grid_point_updates_per_s": 2 * n * n / (us * 1e-6),
+                        "launch_shape": info.launch_shape}
+    return out
+
+
 def run_configs(pb, torch, device):
     """The other configurations: 256^2 FP64 RK4 (1000 steps); 1024^2 FP64 RK4,
     DP45 adaptive (rtol 1e-6) in FP32 and FP64 and the FP32-vs-FP64 error of
@@ -463,26 +493,8 @@ def run_configs(pb, torch, device):
             us, info = _device_us(torch, s, dev, 100)
             out[f"dp45_adaptive_1024_{dtype}"] = {"us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
                                                   "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt}
-    # config 3: 4096^2 TE/TM FP32, ring pump r 20 um w 3 um, delta_LT 0.05, g_pm = -0.2 g_c, dt 0.0015
-    n = 4096
-    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n, dtype=np.float64)
-    X, Y = np.meshgrid(x, x)
-    ring = (1.5 * P_TH * np.exp(-(np.sqrt(X ** 2 + Y ** 2) - 20.0) ** 2 / (2 * 3.0 ** 2))).astype(np.float32)
-    del X, Y
-    rng = np.random.default_rng(4)
-    for dw in (1e-3, 0.0):
-        sp = sysp(n, "f32", dt=0.0015, use_twin_mode=True, stochastic_amplitude=dw, random_seed=4)
-        sp.g_pm, sp.delta_LT = -0.2 * PHYS["g_c"], 0.05
-        with pb.Solver(sp) as s:
-            for comp in ("plus", "minus"):
-                psi0 = (1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
-                s.set_field(f"psi_{comp}", psi0)
-                s.set_field(f"pump_{comp}", ring, 0)
-            s.run(12)
-            us, info = _device_us(torch, s, dev, 20)
-            key = "tetm_4096_f32_noise" if dw else "tetm_4096_f32_deterministic"
-            out[key] = {"us_per_iteration": us, "grid_point_updates_per_s": 2 * n * n / (us * 1e-6),
-                        "launch_shape": info.launch_shape}
+    # config 3: 4096^2 TE/TM FP32
+    out.update(run_tetm(pb, torch, dev, 4096))
     return out
 
 
@@ -510,7 +522,8 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=200, help="timed iterations of the batched sweep")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (inverse-design) leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' timings")
-    ap.add_argument("--only", choices=["configs", "adjoint", "sweep"], help="run one leg alone and print its JSON")
+    ap.add_argument("--only", choices=["configs", "adjoint", "sweep", "tetm"], help="run one leg alone and print its JSON")
+    ap.add_argument("--tetm-n", type=int, default=4096, help="grid of the --only tetm leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -527,7 +540,8 @@ def main():
 
         torch.cuda.set_device(0)
         leg = {"configs": lambda: run_configs(pb, torch, 0), "adjoint": lambda: run_adjoint(pb, torch, 0),
-               "sweep": lambda: run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, 0)}[args.only]
+               "sweep": lambda: run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, 0),
+               "tetm": lambda: run_tetm(pb, torch, 0, args.tetm_n)}[args.only]
         print(json.dumps({args.only: leg()}))
         return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -31,20 +31,24 @@ namespace phx {
 
 // Tile shapes the batch autotuner chooses from: TW x TH points, NT threads.
 // FP64 tiles are half as high (shared memory of the two TMA slots).
-constexpr int kBatchShapes = 3;
+// MINB: CTAs per SM the register allocation leaves room for (the 12-warp
+// shapes run two per SM).
+constexpr int kBatchShapes = 5;
 template <typename T>
 struct BatchShape;
 template <>
 struct BatchShape<float> {
-    static constexpr int TW[kBatchShapes] = {32, 64, 32};
-    static constexpr int TH[kBatchShapes] = {32, 16, 16};
-    static constexpr int NT[kBatchShapes] = {256, 256, 128};
+    static constexpr int TW[kBatchShapes] = {32, 64, 32, 32, 64};
+    static constexpr int TH[kBatchShapes] = {32, 16, 16, 32, 16};
+    static constexpr int NT[kBatchShapes] = {256, 256, 128, 384, 384};
+    static constexpr int MINB[kBatchShapes] = {1, 1, 1, 2, 2};
 };
 template <>
 struct BatchShape<double> {
-    static constexpr int TW[kBatchShapes] = {32, 64, 32};
-    static constexpr int TH[kBatchShapes] = {16, 8, 8};
-    static constexpr int NT[kBatchShapes] = {256, 256, 128};
+    static constexpr int TW[kBatchShapes] = {32, 64, 32, 32, 64};
+    static constexpr int TH[kBatchShapes] = {16, 8, 8, 16, 8};
+    static constexpr int NT[kBatchShapes] = {256, 256, 128, 384, 384};
+    static constexpr int MINB[kBatchShapes] = {1, 1, 1, 2, 2};
 };
 
 struct BatchBase {
@@ -200,8 +204,8 @@ struct BatchEngine final : BatchBase {
         PHX_CUDA(cudaMemcpyAsync(d_inst[S].p, hi.data(), sizeof(BatchInstance<T>) * hi.size(), cudaMemcpyHostToDevice, stream));
         PHX_CUDA(cudaMemcpyAsync(d_tile[S].p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, stream));
         PHX_CUDA(cudaStreamSynchronize(stream));  // host vectors die here
-        auto kern = res ? rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S]>
-                        : rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S]>;
+        auto kern = res ? rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]>
+                        : rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]>;
         const int smem = TmaLayout<T, SH::TW[S], SH::TH[S]>::total;
         PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int per_sm = 0;
@@ -213,6 +217,9 @@ struct BatchEngine final : BatchBase {
         build_one<0>();
         build_one<1>();
         build_one<2>();
+        build_one<3>();
+        build_one<4>();
+        static_assert(kBatchShapes == 5, "every shape needs its tables");
     }
 
     // ------------------------------------------------------------ launches
@@ -226,15 +233,17 @@ struct BatchEngine final : BatchBase {
         B.err = static_cast<int*>(err_flag.p);
         const int smem = TmaLayout<T, SH::TW[S], SH::TH[S]>::total;
         if (res)
-            rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S]><<<blocks[S], SH::NT[S], smem, stream>>>(B);
+            rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]><<<blocks[S], SH::NT[S], smem, stream>>>(B);
         else
-            rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S]><<<blocks[S], SH::NT[S], smem, stream>>>(B);
+            rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]><<<blocks[S], SH::NT[S], smem, stream>>>(B);
     }
     void launch(int sh, int dir) {
         switch (sh) {
             case 0: go<0>(dir); break;
             case 1: go<1>(dir); break;
-            default: go<2>(dir); break;
+            case 2: go<2>(dir); break;
+            case 3: go<3>(dir); break;
+            default: go<4>(dir); break;
         }
         PHX_CUDA(cudaGetLastError());
         ++launches;

@@ -357,8 +357,8 @@ struct BatchParams {
     int* err;
 };
 
-template <typename T, bool RES, int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) rk4_batch_kernel(const __grid_constant__ BatchParams<T> B) {
+template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) rk4_batch_kernel(const __grid_constant__ BatchParams<T> B) {
     auto tile_of = [&](int g) {
         const BatchInstance<T>& I = B.inst[__ldg(B.tile_inst + g)];
         TileRef<T> R;

@@ -63,10 +63,10 @@ def test_batch_matches_oracle_bitwise(require_gpu, dtype):
     with pb.BatchSolver([pb.system_from_case(c) for c, _ in inst]) as b:
         for i, (c, f) in enumerate(inst):
             load_batch(b, i, c, f)
-        i1 = b.run(43)  # 6 tuning iterations, two 16-iteration graphs from plane 0, 5 single launches
+        i1 = b.run(43)  # 10 tuning iterations, two 16-iteration graphs from plane 0, one single launch
         i2 = b.run(37)  # graphs from plane 1
         assert i1.iterations == 43 and i2.iterations == 37
-        assert i1.launch_shape in (0, 1, 2)
+        assert i1.launch_shape in (0, 1, 2, 3, 4)
         for i, (c, f) in enumerate(inst):
             ref, rec = O.run(c, f, max_steps=80)
             assert rec["steps"] == 80
@@ -74,7 +74,7 @@ def test_batch_matches_oracle_bitwise(require_gpu, dtype):
             np.testing.assert_array_equal(b.get_field(i, "n_plus"), np.real(ref["n_plus"]), err_msg=f"instance {i} n")
 
 
-@pytest.mark.parametrize("shape", [0, 1, 2])
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4])
 def test_every_batch_tile_shape_matches_oracle(require_gpu, shape, monkeypatch):
     monkeypatch.setenv("PHX_BATCH_SHAPE", str(shape))
     inst = small_mix("f32")[:3]
