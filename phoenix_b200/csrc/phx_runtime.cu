@@ -120,7 +120,9 @@ struct Engine final : EngineBase {
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + 7];
+    static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
+    static constexpr int kFusedShapes = 9;       // shapes 8-12: persistent TMA-fed variants
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + kFusedShapes];
     static constexpr int kRingBlocks = 64;
     static constexpr int kNormBlocks = 296;
     // imaginary-time propagation (--imagTime): k-stack sums with the complex
@@ -235,8 +237,6 @@ struct Engine final : EngineBase {
     }
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
-    static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
-    static constexpr int kFusedShapes = 7;  // shapes 8-10: persistent TMA-fed variants
     int n_candidates() const { return fused_eligible_static() ? kShapes + kFusedShapes : kShapes; }
     bool is_fused(int sh) const { return sh >= kFusedShape; }
     int cur_shape() const { return shape >= 0 ? shape : tune_step % n_candidates(); }
@@ -670,20 +670,11 @@ struct Engine final : EngineBase {
     int tma_next = 0;
     CUtensorMap tma_pump_map, tma_pot_map;
     int tma_inputs_tw = 0, tma_inputs_th = 0;
-    template <bool RES, int TW, int TH, int NT, int MINB = 1>
-    void go_tma(const FusedParams<T>& F) {
-        using Lay = TmaLayout<T, TW, TH>;
+    // tensor maps and parameters of a TMA iteration with TW x TH tiles
+    template <int TW, int TH>
+    void prepare_tma(TmaParams<T>& Q, const FusedParams<T>& F) {
         static_assert(TW % 4 == 0, "TMA box x alignment needs tile origins on 16-byte boundaries");
-        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT, MINB>;
-        int& tma_blocks_per_sm = tma_blocks[reinterpret_cast<const void*>(kern)];
-        if (!tma_blocks_per_sm) {
-            PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
-            PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_blocks_per_sm, kern, NT, Lay::total));
-            PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
-            if (tma_blocks_per_sm < 1) fail(PHX_ERR_UNSUPPORTED, "TMA iteration kernel does not fit on an SM");
-        }
         if (!err_flag.p) err_flag.alloc(sizeof(int), stream);
-        TmaParams<T> Q;
         std::memset(&Q, 0, sizeof(Q));
         Q.f = F;
         // tensor maps over whole allocations (padded (0,0) = interior (-G,-G));
@@ -716,8 +707,22 @@ struct Engine final : EngineBase {
         Q.has_pump = F.pump != nullptr;
         Q.has_pot = F.pot != nullptr;
         Q.tiles_x = (N_c + TW - 1) / TW;
-        Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
         Q.err = static_cast<int*>(err_flag.p);
+        if (!sm_count) PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
+    }
+    template <bool RES, int TW, int TH, int NT, int MINB = 1>
+    void go_tma(const FusedParams<T>& F) {
+        using Lay = TmaLayout<T, TW, TH>;
+        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT, MINB>;
+        int& tma_blocks_per_sm = tma_blocks[reinterpret_cast<const void*>(kern)];
+        if (!tma_blocks_per_sm) {
+            PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
+            PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_blocks_per_sm, kern, NT, Lay::total));
+            if (tma_blocks_per_sm < 1) fail(PHX_ERR_UNSUPPORTED, "TMA iteration kernel does not fit on an SM");
+        }
+        TmaParams<T> Q;
+        prepare_tma<TW, TH>(Q, F);
+        Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
         const int blocks = std::min(Q.n_tiles, tma_blocks_per_sm * sm_count);
         kern<<<blocks, NT, Lay::total, stream>>>(Q);
     }
@@ -739,6 +744,9 @@ struct Engine final : EngineBase {
             // 12 warps per CTA, two CTAs per SM: registers capped at 85
             case 5: go_tma<RES, 32, f32 ? 32 : 16, 384, 2>(F); return;
             case 6: go_tma<RES, 64, f32 ? 16 : 8, 384, 2>(F); return;
+            // taller tiles, one CTA per SM: less halo recomputation per output point
+            case 7: go_tma<RES, 64, f32 ? 32 : 16, 768>(F); return;
+            case 8: go_tma<RES, 64, f32 ? 32 : 16, 512>(F); return;
             default: break;
         }
         switch (cur_shape() - kFusedShape) {

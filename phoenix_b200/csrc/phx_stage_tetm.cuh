@@ -70,15 +70,20 @@ __device__ __forceinline__ void neighbours(const Row<T>& r, int lane, cx<T>* L, 
 }
 
 // Both polarisations at one point: k of psi+, n+, psi-, n-; the pointwise
-// inputs come from `src` (TetmGlobalSrc or a shared-memory copy)
+// inputs come from `src` (TetmGlobalSrc or a shared-memory copy).  The
+// reference multiplies complex numbers whose imaginary part is exactly zero
+// (the reservoir, stored real here) or whose real part is (half_i / dx / dy),
+// and multiplies by -1 to negate; this keeps only the products that are not
+// with that zero and negates directly, which changes no result except,
+// possibly, the sign of an exact zero.
 template <typename T, typename Src>
 __device__ __forceinline__ void rhs_tetm_src(const TetmParams<T>& Q, const Src& src, cx<T> wp, cx<T> upp, cx<T> dnp, cx<T> lp,
                                              cx<T> rp, cx<T> ulp, cx<T> urp, cx<T> dlp, cx<T> drp, cx<T> wm, cx<T> upm,
                                              cx<T> dnm, cx<T> lm, cx<T> rm, cx<T> ulm, cx<T> urm, cx<T> dlm, cx<T> drm, T rvp,
                                              T rvm, cx<T>& kwp, T& krp, cx<T>& kwm, T& krm) {
     const StageParams<T>& P = Q.p;
-    const cx<T> in_wf_plus_mi = mk(wp.im, rmul((T)-1.0, wp.re));
-    const cx<T> in_wf_minus_mi = mk(wm.im, rmul((T)-1.0, wm.re));
+    const cx<T> in_wf_plus_mi = mk(wp.im, -wp.re);
+    const cx<T> in_wf_minus_mi = mk(wm.im, -wm.re);
     const cx<T> horizontal_plus = smul(P.odx2, cadd(rp, lp));
     const cx<T> vertical_plus = smul(P.ody2, cadd(dnp, upp));
     const cx<T> horizontal_minus = smul(P.odx2, cadd(rm, lm));
@@ -86,16 +91,16 @@ __device__ __forceinline__ void rhs_tetm_src(const TetmParams<T>& Q, const Src& 
     // psi[i+ro+1] + psi[i-ro-1] - psi[i+ro-1] - psi[i-ro+1]
     const cx<T> diag_m = csub(csub(cadd(drm, ulm), dlm), urm);
     const cx<T> diag_p = csub(csub(cadd(drp, ulp), dlp), urp);
-    cx<T> hcp = cadd(csub(horizontal_minus, vertical_minus), cmul(Q.hidd, diag_m));
-    cx<T> hcm = csub(csub(horizontal_plus, vertical_plus), cmul(Q.hidd, diag_p));
+    // hidd = (0, h): (0 a - h b, 0 b + h a) = (-h b, h a)
+    cx<T> hcp = cadd(csub(horizontal_minus, vertical_minus), mk(-rmul(Q.hidd.im, diag_m.im), rmul(Q.hidd.im, diag_m.re)));
+    cx<T> hcm = csub(csub(horizontal_plus, vertical_plus), mk(-rmul(Q.hidd.im, diag_p.im), rmul(Q.hidd.im, diag_p.re)));
     cx<T> hrp = cadd(cadd(smul(P.m2, wp), horizontal_plus), vertical_plus);
     cx<T> hrm = cadd(cadd(smul(P.m2, wm), horizontal_minus), vertical_minus);
     const T npl = abs2(wp), nmi = abs2(wm);
-    hrp = mk(hrp.im, rmul((T)-1.0, hrp.re));
-    hrm = mk(hrm.im, rmul((T)-1.0, hrm.re));
-    hcp = mk(hcp.im, rmul((T)-1.0, hcp.re));
-    hcm = mk(hcm.im, rmul((T)-1.0, hcm.re));
-    const cx<T> rvp_c = mk(rvp, (T)0), rvm_c = mk(rvm, (T)0);
+    hrp = mk(hrp.im, -hrp.re);
+    hrm = mk(hrm.im, -hrm.re);
+    hcp = mk(hcp.im, -hcp.re);
+    hcm = mk(hcm.im, -hcm.re);
 
     // wavefunction plus
     cx<T> res = smul(Q.ohb_meff, hrp);
@@ -104,8 +109,8 @@ __device__ __forceinline__ void rhs_tetm_src(const TetmParams<T>& Q, const Src& 
         res = cadd(res, cmul(smul(P.ohb, pot), in_wf_plus_mi));
     }
     res = cadd(res, smul(rmul(P.ohb_gc, npl), in_wf_plus_mi));
-    res = cadd(res, cmul(smul(P.ohb_gr, rvp_c), in_wf_plus_mi));
-    res = cadd(res, cmul(smul(P.half_R, rvp_c), wp));
+    res = cadd(res, smul(rmul(P.ohb_gr, rvp), in_wf_plus_mi));
+    res = cadd(res, smul(rmul(P.half_R, rvp), wp));
     res = csub(res, smul(P.half_gamma_c, wp));
     res = cadd(res, smul(rmul(Q.ohb_gpm, nmi), in_wf_plus_mi));
     res = cadd(res, smul(Q.ohb_dlt, hcp));
@@ -124,8 +129,8 @@ __device__ __forceinline__ void rhs_tetm_src(const TetmParams<T>& Q, const Src& 
         res = cadd(res, cmul(smul(P.ohb, pot), in_wf_minus_mi));
     }
     res = cadd(res, smul(rmul(P.ohb_gc, nmi), in_wf_minus_mi));
-    res = cadd(res, cmul(smul(P.ohb_gr, rvm_c), in_wf_minus_mi));
-    res = cadd(res, cmul(smul(P.half_R, rvm_c), wm));
+    res = cadd(res, smul(rmul(P.ohb_gr, rvm), in_wf_minus_mi));
+    res = cadd(res, smul(rmul(P.half_R, rvm), wm));
     res = csub(res, smul(P.half_gamma_c, wm));
     res = cadd(res, smul(rmul(Q.ohb_gpm, npl), in_wf_minus_mi));
     res = cadd(res, smul(Q.ohb_dlt, hcm));

@@ -19,7 +19,9 @@
 //
 // Every wait on an mbarrier is bounded: when it gives up the CTA sets the
 // error flag, waits (again bounded) for the load it may still have in
-// flight and leaves; the host turns the flag into PHX_ERR_TIMEOUT.
+// flight and leaves; the host turns the flag into PHX_ERR_TIMEOUT.  Only
+// thread 0 polls the mbarrier; the other threads wait at the CTA barrier
+// that follows.
 #pragma once
 
 #include <cuda.h>
@@ -211,7 +213,10 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
             int* dst = reinterpret_cast<int*>(&sP);
             for (int w = threadIdx.x; w < kWords; w += NT) dst[w] = __ldg(src + w);
         }
-        const bool ok = mbar_wait_bounded(&bars[slot], parity);
+        // thread 0 waits for the tile's boxes; the others wait at the barrier
+        // (no issue slots spent spinning), which also orders the data thread 0
+        // observed before their reads
+        const bool ok = threadIdx.x == 0 ? mbar_wait_bounded(&bars[slot], parity) : true;
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicExch(err, 1);
