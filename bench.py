@@ -15,7 +15,8 @@ Legs of the JSON line:
   e2e        the same workload through the public API with host buffers:
              upload psi0/n0 from pinned host memory, run in chunks of 100
              iterations reading the FP64 norm back after each chunk, download
-             psi and n into pinned host memory at the end
+             psi and n into pinned host memory at the end (after one untimed
+             pass of the same sequence on the same handle and buffers)
   roofline   the dominant kernel (fused RK4 stage 2/3) from per-launch CUDA
              events recorded by the library on its stream during the timed
              region: algorithmic bytes / average duration vs measured HBM peak
@@ -648,20 +649,27 @@ def main():
     s2.set_field("fft_mask_plus", wl["mask"])
     torch.cuda.synchronize()
     st2 = torch.cuda.ExternalStream(s2.stream, device=local)
+
+    def end_to_end(iters):
+        """upload the inputs from pinned host memory, iterate with an FP64 norm
+        read back every `chunk` iterations, download the state"""
+        s2.set_field("psi_plus", pinned_psi)
+        s2.set_field("n_plus", pinned_n)
+        done, norms = 0, []
+        while done < iters:
+            k = min(chunk, iters - done)
+            s2.run(k)
+            norms.append(s2.sum_abs2("psi_plus"))
+            done += k
+        return s2.get_field("psi_plus", out=pinned_psi_out), s2.get_field("n_plus", out=pinned_n_out), norms
+
+    # untimed pass: first use of the pinned buffers and of the handle's planes
+    end_to_end(min(chunk, e2e_iters))
+    torch.cuda.synchronize()
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(st2):
         a0.record(st2)
-    s2.set_field("psi_plus", pinned_psi)
-    s2.set_field("n_plus", pinned_n)
-    done = 0
-    norms = []
-    while done < e2e_iters:
-        k = min(chunk, e2e_iters - done)
-        s2.run(k)
-        norms.append(s2.sum_abs2("psi_plus"))
-        done += k
-    psi_out = s2.get_field("psi_plus", out=pinned_psi_out)
-    n_out = s2.get_field("n_plus", out=pinned_n_out)
+    psi_out, n_out, norms = end_to_end(e2e_iters)
     with torch.cuda.stream(st2):
         a1.record(st2)
     torch.cuda.synchronize()

@@ -20,7 +20,9 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <array>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "../../include/phx.h"
@@ -226,6 +228,11 @@ struct Engine final : EngineBase {
             if (v >= 0 && v < kShapes) shape = v;
             if (v >= kFusedShape && v < kFusedShape + kFusedShapes && fused_eligible_static()) shape = v;
         }
+        if (shape < 0 && tune_cache_on()) {
+            std::lock_guard<std::mutex> lk(tune_cache_mu());
+            auto it = tune_cache().find(tune_key());
+            if (it != tune_cache().end()) shape = it->second;
+        }
         partials.alloc(sizeof(double) * 2 * std::max<long long>(max_blocks, 1024), stream);
         result.alloc(sizeof(double) * 4, stream);
         host_result.alloc(sizeof(double) * 4);
@@ -237,9 +244,13 @@ struct Engine final : EngineBase {
     }
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
-    int n_candidates() const { return fused_eligible_static() ? kShapes + kFusedShapes : kShapes; }
+    // autotuning candidates: the stage kernels' shapes 0-3, or, where the
+    // one-kernel iteration applies, its shapes 4-12 (the stage kernels, four
+    // launches and 236 B per point, never beat it there)
+    int first_candidate() const { return fused_eligible_static() ? kFusedShape : 0; }
+    int n_candidates() const { return fused_eligible_static() ? kFusedShapes : kShapes; }
     bool is_fused(int sh) const { return sh >= kFusedShape; }
-    int cur_shape() const { return shape >= 0 ? shape : tune_step % n_candidates(); }
+    int cur_shape() const { return shape >= 0 ? shape : first_candidate() + tune_step % n_candidates(); }
     // the fused iteration handles scalar RK4 with at most one pump and one
     // potential group and no pulse (real temporal coefficients are checked
     // every iteration)
@@ -1545,10 +1556,31 @@ struct Engine final : EngineBase {
         }
     }
 
-    // Launch-shape autotuning: the first 2*kShapes iterations of a handle run
-    // with each shape twice (results do not depend on the shape: every point
-    // is computed by the same operations); the second round is timed and the
-    // fastest shape is kept.
+    // Launch-shape autotuning: the first 2 x (candidates) iterations of a
+    // handle run each candidate shape twice (results do not depend on the
+    // shape: every point is computed by the same operations); the second round
+    // is timed and the fastest shape is kept, and remembered for the process:
+    // a later handle of the same configuration (grid, precision, boundaries,
+    // inputs, iterator, device) starts with it.  PHX_TUNE_CACHE=0 turns the
+    // memory off.
+    static bool tune_cache_on() {
+        const char* e = std::getenv("PHX_TUNE_CACHE");
+        return !(e && e[0] == '0');
+    }
+    using TuneKey = std::array<long long, 14>;
+    static std::map<TuneKey, int>& tune_cache() {
+        static std::map<TuneKey, int> m;
+        return m;
+    }
+    static std::mutex& tune_cache_mu() {
+        static std::mutex mu;
+        return mu;
+    }
+    TuneKey tune_key() const {
+        return {(long long)sizeof(T), N_r, N_c, P.use_reservoir, P.n_pump_groups, P.n_potential_groups,
+                P.n_pulse_groups, P.periodic_x, P.periodic_y, P.iterator, P.tetm, P.device,
+                (long long)(P.stochastic_amplitude > 0.0), (long long)imag_time()};
+    }
     void tune_record(cudaEvent_t ta, cudaEvent_t tb) {
         tb = get_event();
         PHX_CUDA(cudaEventRecord(tb, stream));
@@ -1565,7 +1597,7 @@ struct Engine final : EngineBase {
                 PHX_CUDA(cudaEventElapsedTime(&m, tune_ev[sh][i].first, tune_ev[sh][i].second));
                 ms = std::min(ms, m);
             }
-            if (ms < best) best = ms, best_sh = sh;
+            if (ms < best) best = ms, best_sh = first_candidate() + sh;
             for (auto& pr : tune_ev[sh]) {
                 event_pool.push_back(pr.first);
                 event_pool.push_back(pr.second);
@@ -1573,6 +1605,10 @@ struct Engine final : EngineBase {
             tune_ev[sh].clear();
         }
         shape = best_sh;
+        if (tune_cache_on()) {
+            std::lock_guard<std::mutex> lk(tune_cache_mu());
+            tune_cache()[tune_key()] = shape;
+        }
     }
 
     // ------------------------------------------------------------ device-pointer field I/O

@@ -227,11 +227,12 @@ def test_tma_iterations_on_ragged_grids(require_gpu, monkeypatch, dtype, px, py)
 
 
 def test_autotuning_across_every_shape_is_bit_identical(require_gpu, monkeypatch):
-    """The first iterations of a handle cycle through every launch shape (TMA
-    tile shapes of different sizes among them, whose tensor maps differ): the
-    result equals a run on one fixed shape."""
+    """The first iterations of a handle cycle through every candidate launch
+    shape (TMA tile shapes of different sizes among them, whose tensor maps
+    differ): the result equals a run on one fixed shape."""
     import bench as B
 
+    monkeypatch.setenv("PHX_TUNE_CACHE", "0")  # tune in this handle, whatever ran before
     n = 256
     wl = B.workload(n)
     outs = []
@@ -253,6 +254,31 @@ def test_autotuning_across_every_shape_is_bit_identical(require_gpu, monkeypatch
             outs.append((s.get_field("psi_plus"), s.get_field("n_plus")))
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
     np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
+def test_tuned_shape_is_remembered_per_configuration(require_gpu, monkeypatch):
+    """A second handle of the same configuration starts with the shape the
+    first one tuned (no tuning iterations); another grid tunes anew; with
+    PHX_TUNE_CACHE=0 every handle tunes."""
+    import bench as B
+
+    monkeypatch.delenv("PHX_STAGE_SHAPE", raising=False)
+
+    def first_shape(n):
+        sp = B.system(pb, n, "f32", 0)
+        sp.fft_every = 1e12
+        with pb.Solver(sp) as s:
+            s.set_field("psi_plus", np.zeros((n, n)))
+            first = s.run(1).launch_shape
+            last = s.run(29).launch_shape
+        return first, last
+
+    tuned = first_shape(192)[1]
+    assert tuned >= 4
+    assert first_shape(192) == (tuned, tuned)
+    assert first_shape(200)[0] == -1
+    monkeypatch.setenv("PHX_TUNE_CACHE", "0")
+    assert first_shape(192)[0] == -1
 
 
 def test_bad_field_shape_is_rejected(require_gpu):
