@@ -213,8 +213,9 @@ __device__ __forceinline__ void adj_images4(int N_r, int N_c, long long pitch, V
     if ((lx || hx) && (ly || hy)) base[(long long)rs * pitch + cs] = v;
 }
 
-template <typename T, int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) adj_fused_kernel(const __grid_constant__ AdjFusedParams<T> Q) {
+// MINB: CTAs per SM the register allocation must leave room for
+template <typename T, int TW, int TH, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) adj_fused_kernel(const __grid_constant__ AdjFusedParams<T> Q) {
     constexpr int W4 = TW + 8, H4 = TH + 8;  // lam' with a 4-cell halo
     constexpr int W3 = TW + 6, H3 = TH + 6;  // Ybar regions (3-cell halo at most)
     constexpr int NP = W3 * H3;
@@ -244,6 +245,23 @@ __global__ void __launch_bounds__(NT) adj_fused_kernel(const __grid_constant__ A
         const cx<T>* prev = sB[(s + 1) & 1];
         cx<T>* cur = sB[s & 1];
         const T dtb = Q.dt_b[s - 1], adt = s < 4 ? Q.a_dt[s - 1] : (T)0;
+        // this stage's global values of every owned point, loaded before any
+        // arithmetic so that the loads are in flight together
+        cx<T> ypsi[OWN];
+        T yn[OWN], lamn[OWN], potv[OWN];
+#pragma unroll
+        for (int j = 0; j < OWN; ++j) {
+            const int q = threadIdx.x + NT * j;
+            const int qy = q / W3, qx = q - qy * W3;
+            const int dy = qy - 3, dx = qx - 3;
+            const int r = ty0 + dy, c = tx0 + dx;
+            const bool live = q < NP && dy >= -h && dy < TH + h && dx >= -h && dx < TW + h && r < Q.N_r + 4 && c < Q.N_c + 4;
+            const long long i = (long long)r * p + c;
+            ypsi[j] = live ? Q.Ypsi[s - 1][i] : mk((T)0, (T)0);
+            yn[j] = (live && Q.res) ? Q.Yn[s - 1][i] : (T)0;
+            lamn[j] = (live && Q.res) ? Q.lam_n[i] : (T)0;
+            potv[j] = (live && Q.pot) ? Q.pot[i] : (T)0;
+        }
         auto mu_at = [&](int qy, int qx) {  // kbar_s psi at W3-grid point (qy, qx) (may be a halo-4 point)
             cx<T> m = sL[(qy + 1) * W4 + qx + 1];
             m.re *= dtb;
@@ -268,7 +286,6 @@ __global__ void __launch_bounds__(NT) adj_fused_kernel(const __grid_constant__ A
                 ybn[j] = (T)0;
                 continue;
             }
-            const long long i = (long long)r * p + c;
             const cx<T> mu = mu_at(qy, qx);
             // neighbours: stage 4 reads lam' only (halo 4 in sL); lower stages read Ybar_{s+1}
             // on its region, one cell wider than this one
@@ -285,9 +302,9 @@ __global__ void __launch_bounds__(NT) adj_fused_kernel(const __grid_constant__ A
                 mu_u = mu_at(qy - 1, qx), mu_d = mu_at(qy + 1, qx), mu_l = mu_at(qy, qx - 1), mu_r = mu_at(qy, qx + 1);
             }
             T m = (T)0;
-            if (Q.res) m = dtb * Q.lam_n[i] + adt * ybn[j];
-            const cx<T> psi = Q.Ypsi[s - 1][i];
-            const T n = Q.res ? Q.Yn[s - 1][i] : (T)0;
+            if (Q.res) m = dtb * lamn[j] + adt * ybn[j];
+            const cx<T> psi = ypsi[j];
+            const T n = yn[j];
             const T norm = psi.re * psi.re + psi.im * psi.im;
             cx<T> lap;
             lap.re = Q.m2 * mu.re + Q.ody2 * (mu_u.re + mu_d.re) + Q.odx2 * (mu_l.re + mu_r.re);
@@ -298,7 +315,7 @@ __global__ void __launch_bounds__(NT) adj_fused_kernel(const __grid_constant__ A
                 W += Q.ohb_gr * n;
                 B += Q.half_R * n;
             }
-            if (Q.pot) W += Q.ohb * (Q.pot[i] * Q.c_pot[s - 1]);
+            if (Q.pot) W += Q.ohb * (potv[j] * Q.c_pot[s - 1]);
             const T hre = Q.A * lap.re + W * mu.re, him = Q.A * lap.im + W * mu.im;
             const T im_mbar_psi = mu.re * psi.im - mu.im * psi.re;
             const T re_mbar_psi = mu.re * psi.re + mu.im * psi.im;

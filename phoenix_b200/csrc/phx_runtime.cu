@@ -20,6 +20,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <array>
 #include <map>
 #include <mutex>
@@ -1654,6 +1655,8 @@ struct Engine final : EngineBase {
     // one fused launch per iteration (adj_fused_kernel); PHX_ADJOINT_STAGES=1
     // selects the four-launch path (adj_stage_kernel)
     bool adj_fused = !(std::getenv("PHX_ADJOINT_STAGES") && std::atoi(std::getenv("PHX_ADJOINT_STAGES")) == 1);
+    bool adj_recompute_tma =
+        !(std::getenv("PHX_ADJOINT_RECOMPUTE") && std::string(std::getenv("PHX_ADJOINT_RECOMPUTE")) == "fused");
 
     void adjoint_check() {
         if (P.iterator != PHX_ITER_RK4 || P.tetm) fail(PHX_ERR_UNSUPPORTED, "the adjoint covers scalar fixed-step RK4");
@@ -1734,8 +1737,51 @@ struct Engine final : EngineBase {
                 launch<kRk4Last>(S, wire);
         }
     }
+    // The recompute's TMA iteration: the state planes change from one
+    // iteration to the next; the launch's parameters carry their tensor maps.
+    std::map<std::pair<const void*, bool>, CUtensorMap> store_maps;
+    template <bool RES, int TW, int TH, int NT, int MINB>
+    void go_tma_store(const FusedParams<T>& F, DevBuf& yp, DevBuf* yn) {
+        using Lay = TmaLayout<T, TW, TH>;
+        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT, MINB, true>;
+        int& blocks_per_sm = tma_blocks[reinterpret_cast<const void*>(kern)];
+        if (!blocks_per_sm) {
+            PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
+            PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, NT, Lay::total));
+            if (blocks_per_sm < 1) fail(PHX_ERR_UNSUPPORTED, "TMA iteration kernel does not fit on an SM");
+        }
+        if (!err_flag.p) err_flag.alloc(sizeof(int), stream);
+        if (!sm_count) PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
+        // a map depends only on the plane's address and on whether it is
+        // complex (pitch, rows and the boxes are fixed for this handle and
+        // this kernel), so encodings are kept per plane
+        auto map_of = [&](const void* base, bool complex, int box_h) -> const CUtensorMap& {
+            auto it = store_maps.find({base, complex});
+            if (it == store_maps.end()) {
+                CUtensorMap m;
+                tensor_map(&m, const_cast<void*>(base), complex, TW + 8, box_h);
+                it = store_maps.emplace(std::make_pair(base, complex), m).first;
+            }
+            return it->second;
+        };
+        TmaParams<T> Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.f = F;
+        Q.psi_map = map_of(yp.p, true, TH + 8);
+        if (RES) Q.n_map = map_of(yn->p, false, TH + 6);
+        if (F.pump) Q.pump_map = map_of(pump[0].p, false, TH + 6);
+        if (F.pot) Q.pot_map = map_of(pot[0].p, false, TH + 6);
+        Q.has_pump = F.pump != nullptr;
+        Q.has_pot = F.pot != nullptr;
+        Q.tiles_x = (N_c + TW - 1) / TW;
+        Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
+        Q.err = static_cast<int*>(err_flag.p);
+        const int blocks = std::min(Q.n_tiles, blocks_per_sm * sm_count);
+        kern<<<blocks, NT, Lay::total, stream>>>(Q);
+    }
     // the same in one launch: the fused iteration kernel that also stores the
-    // stage values (bit-identical to the stage kernels)
+    // stage values (bit-identical to the stage kernels); the TMA-fed iteration
+    // by default, rk4_fused_kernel with PHX_ADJOINT_RECOMPUTE=fused
     void rk4_recompute_fused(DevBuf& yp, DevBuf* yn, DevBuf* sp[3], DevBuf* sn[3], DevBuf& op, DevBuf* on) {
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
         FusedParams<T> F;
@@ -1755,14 +1801,24 @@ struct Engine final : EngineBase {
             F.st_psi[s] = cplane(*sp[s]);
             F.st_n[s] = sn[s] ? rplane(*sn[s]) : nullptr;
         }
-        constexpr int TW = 32, TH = sizeof(T) == 4 ? 32 : 16;
-        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
         cudaEvent_t a = nullptr;
         prof_begin(a);
-        if (P.use_reservoir)
-            rk4_fused_kernel<T, true, TW, TH, 256, true><<<grid, 256, 0, stream>>>(F);
-        else
-            rk4_fused_kernel<T, false, TW, TH, 256, true><<<grid, 256, 0, stream>>>(F);
+        if (adj_recompute_tma) {
+            // FP32: 64 x 16 tiles, 12 warps, two CTAs per SM; FP64: 64 x 16
+            // tiles, 24 warps, one CTA per SM (no register spills)
+            constexpr int NT = sizeof(T) == 4 ? 384 : 768, MINB = sizeof(T) == 4 ? 2 : 1;
+            if (P.use_reservoir)
+                go_tma_store<true, 64, 16, NT, MINB>(F, yp, yn);
+            else
+                go_tma_store<false, 64, 16, NT, MINB>(F, yp, yn);
+        } else {
+            constexpr int TW = 32, TH = sizeof(T) == 4 ? 32 : 16;
+            dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+            if (P.use_reservoir)
+                rk4_fused_kernel<T, true, TW, TH, 256, true><<<grid, 256, 0, stream>>>(F);
+            else
+                rk4_fused_kernel<T, false, TW, TH, 256, true><<<grid, 256, 0, stream>>>(F);
+        }
         const double st = sizeof(C) + (P.use_reservoir ? sizeof(T) : 0);
         prof_end(PHX_KERNEL_RK4_FUSED, a, (double)N_r * N_c * (5 * st + (P.n_pump_groups ? sizeof(T) : 0)));
         ++launches;
@@ -1863,11 +1919,21 @@ struct Engine final : EngineBase {
                     Q.odx2 = d.odx2;
                     Q.ody2 = d.ody2;
                     Q.res = res;
-                    constexpr int TW = 32, TH = 16;
-                    dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
                     cudaEvent_t a = nullptr;
                     prof_begin(a);
-                    adj_fused_kernel<T, TW, TH, 256><<<grid, 256, 0, stream>>>(Q);
+                    auto go_adj = [&](auto tw, auto th, auto nt, auto minb) {
+                        constexpr int TW = decltype(tw)::value, TH = decltype(th)::value, NT = decltype(nt)::value;
+                        constexpr int MINB = decltype(minb)::value;
+                        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+                        adj_fused_kernel<T, TW, TH, NT, MINB><<<grid, NT, 0, stream>>>(Q);
+                    };
+                    using std::integral_constant;
+                    if constexpr (sizeof(T) == 4)  // 64 x 16 tiles, 16 warps, two CTAs per SM
+                        go_adj(integral_constant<int, 64>{}, integral_constant<int, 16>{}, integral_constant<int, 512>{},
+                               integral_constant<int, 2>{});
+                    else
+                        go_adj(integral_constant<int, 32>{}, integral_constant<int, 16>{}, integral_constant<int, 256>{},
+                               integral_constant<int, 1>{});
                     prof_end(PHX_KERNEL_OTHER, a, (double)N_r * N_c * (5.0 * sizeof(C) + 7.0 * sizeof(T)));
                     ++launches;
                     PHX_CUDA(cudaGetLastError());
@@ -1932,6 +1998,7 @@ struct Engine final : EngineBase {
         }
         PHX_CUDA(cudaGetLastError());
         PHX_CUDA(cudaStreamSynchronize(stream));  // scratch planes are freed on return
+        check_err_flag();
     }
 
     double sum_abs2(int field) override {

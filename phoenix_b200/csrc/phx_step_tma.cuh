@@ -147,7 +147,7 @@ struct TileRef {
 // tensor maps and parameters live in global memory (one set per instance);
 // the maps are acquired for the tensor-map proxy before use and the tile's
 // parameters are staged in shared memory.
-template <typename T, bool RES, int TW, int TH, int NT, bool BATCH, typename TileOf>
+template <typename T, bool RES, int TW, int TH, int NT, bool BATCH, bool STORE, typename TileOf>
 __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles, int* err) {
     using Lay = TmaLayout<T, TW, TH>;
     constexpr int W4 = Lay::W4, WR = Lay::WR;
@@ -296,6 +296,18 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
                     if (s < 3) {
                         o[h] = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
                         if constexpr (RES) ns[j][h] = radd(n0[j][h], rmul(P.dtw[s], kr[h]));
+                        if constexpr (STORE) {
+                            const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
+                            if (qy >= 3 && qy < H3 - 3 && qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {
+                                const long long g = (long long)gy * pitch + gx;
+                                P.st_psi[s][g] = o[h];
+                                if (P.img_x | P.img_y) fused_images(P, P.st_psi[s], gy, gx, o[h]);
+                                if constexpr (RES) {
+                                    P.st_n[s][g] = ns[j][h];
+                                    if (P.img_x | P.img_y) fused_images(P, P.st_n[s], gy, gx, ns[j][h]);
+                                }
+                            }
+                        }
                     } else {
                         const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
                         if (qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {
@@ -322,8 +334,10 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
     }
 }
 
-// MINB: CTAs per SM the register allocation must leave room for
-template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1>
+// MINB: CTAs per SM the register allocation must leave room for.  STORE: also
+// write the stage values Y2..Y4 of the tile's points (f.st_psi / f.st_n, with
+// periodic images), which the adjoint's backward sweep reads.
+template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1, bool STORE = false>
 __global__ void __launch_bounds__(NT, MINB) rk4_tma_kernel(const __grid_constant__ TmaParams<T> Q) {
     auto tile_of = [&](int g) {
         TileRef<T> R;
@@ -338,7 +352,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_tma_kernel(const __grid_constant
         R.tx0 = (g % Q.tiles_x) * TW;
         return R;
     };
-    tma_tile_loop<T, RES, TW, TH, NT, false>(tile_of, Q.n_tiles, Q.err);
+    tma_tile_loop<T, RES, TW, TH, NT, false, STORE>(tile_of, Q.n_tiles, Q.err);
 }
 
 // ---------------------------------------------------------------- batches
@@ -379,7 +393,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_batch_kernel(const __grid_consta
         R.tx0 = (local % I.tiles_x) * TW;
         return R;
     };
-    tma_tile_loop<T, RES, TW, TH, NT, true>(tile_of, B.n_tiles, B.err);
+    tma_tile_loop<T, RES, TW, TH, NT, true, false>(tile_of, B.n_tiles, B.err);
 }
 
 }  // namespace phx
