@@ -1737,6 +1737,30 @@ struct Engine final : EngineBase {
                 launch<kRk4Last>(S, wire);
         }
     }
+    // storing variants of the non-TMA one-kernel shapes (go_fused's cases 0-3);
+    // false when the tuned shape is not one of them
+    template <bool RES, int TW, int TH, int NT>
+    void go_fused_shape_store(const FusedParams<T>& F) {
+        dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
+        rk4_fused_kernel<T, RES, TW, TH, NT, true><<<grid, NT, 0, stream>>>(F);
+    }
+    template <bool RES>
+    bool go_fused_store_tuned(const FusedParams<T>& F) {
+        constexpr bool f32 = sizeof(T) == 4;
+        if (!is_fused(cur_shape())) return false;
+        switch (cur_shape() - kFusedShape) {
+            case 0: go_fused_shape_store<RES, 32, f32 ? 32 : 16, 256>(F); return true;
+            case 1: go_fused_shape_store<RES, 64, f32 ? 16 : 8, 256>(F); return true;
+            case 2: go_fused_shape_store<RES, 32, f32 ? 16 : 8, 128>(F); return true;
+            case 3:
+                if constexpr (f32)
+                    go_fused_shape_store<RES, 64, 32, 512>(F);
+                else
+                    go_fused_shape_store<RES, 32, 24, 384>(F);
+                return true;
+            default: return false;
+        }
+    }
     // The recompute's TMA iteration: the state planes change from one
     // iteration to the next; the launch's parameters carry their tensor maps.
     std::map<std::pair<const void*, bool>, CUtensorMap> store_maps;
@@ -1804,12 +1828,16 @@ struct Engine final : EngineBase {
         cudaEvent_t a = nullptr;
         prof_begin(a);
         if (adj_recompute_tma) {
-            // FP32: 64 x 16 tiles, 12 warps, two CTAs per SM; FP64: 64 x 16
-            // tiles, 24 warps, one CTA per SM (no register spills)
+            // the forward's tuned one-kernel shape when it is a non-TMA one (small
+            // grids, where the TMA kernel's few large CTAs leave SMs idle);
+            // otherwise the TMA iteration -- FP32: 64 x 16 tiles, 12 warps, two
+            // CTAs per SM; FP64: 64 x 16 tiles, 24 warps, one CTA per SM (no
+            // register spills)
+            const bool done = P.use_reservoir ? go_fused_store_tuned<true>(F) : go_fused_store_tuned<false>(F);
             constexpr int NT = sizeof(T) == 4 ? 384 : 768, MINB = sizeof(T) == 4 ? 2 : 1;
-            if (P.use_reservoir)
+            if (!done && P.use_reservoir)
                 go_tma_store<true, 64, 16, NT, MINB>(F, yp, yn);
-            else
+            else if (!done)
                 go_tma_store<false, 64, 16, NT, MINB>(F, yp, yn);
         } else {
             constexpr int TW = 32, TH = sizeof(T) == 4 ? 32 : 16;
