@@ -411,8 +411,9 @@ def run_adjoint(pb, torch, device, iters=500, n=512):
             "kernels_forward_and_backward": kernels,
             "plain_forward_ms": plain_ms, "checkpointed_forward_ms": fwd, "backward_ms": bwd,
             "backward_over_plain_forward": bwd / plain_ms,
-            "note": "backward = per iteration one fused recompute launch (stage values stored) + one fused "
-                    "vector-Jacobian launch; loss evaluation by torch between the two"}
+            "note": "backward = per iteration one fused recompute launch (stage values stored, on a second "
+                    "stream, one segment ahead) + one fused vector-Jacobian launch; loss evaluation by torch "
+                    "between the two"}
 
 
 def _device_us(torch, solver, device, iters):

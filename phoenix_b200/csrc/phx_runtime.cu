@@ -1648,6 +1648,7 @@ struct Engine final : EngineBase {
     std::vector<std::unique_ptr<DevBuf>> ck_psi, ck_n;    // checkpoints (state planes)
     std::vector<std::unique_ptr<DevBuf>> sg_psi, sg_n;    // states of one segment
     std::vector<std::unique_ptr<DevBuf>> st_psi, st_n;    // Y2..Y4 of every iteration of a segment
+    std::vector<std::unique_ptr<DevBuf>> sg_psi2, sg_n2, st_psi2, st_n2;  // the second set (overlapped recompute)
     DevBuf lam_psi[2], lam_n[2], yb_psi[2], yb_n[2], la_psi, la_n, pbar;
     int64_t adj_T = 0, adj_every = 0;
     T adj_dt = 0;
@@ -1865,6 +1866,14 @@ struct Engine final : EngineBase {
             ensure_planes(sg_n, (size_t)every + 1, rb);
             ensure_planes(st_n, (size_t)(3 * every), rb);
         }
+        if (adj_fused && nck > 1) {
+            ensure_planes(sg_psi2, (size_t)every + 1, cb);
+            ensure_planes(st_psi2, (size_t)(3 * every), cb);
+            if (res) {
+                ensure_planes(sg_n2, (size_t)every + 1, rb);
+                ensure_planes(st_n2, (size_t)(3 * every), rb);
+            }
+        }
         for (int b = 0; b < 2; ++b) {
             if (!lam_psi[b].p) lam_psi[b].alloc(cb, stream);
             if (!yb_psi[b].p) yb_psi[b].alloc(cb, stream);
@@ -1895,21 +1904,78 @@ struct Engine final : EngineBase {
         const T bw[4] = {(T)(1.0 / 6.0), (T)(1.0 / 3.0), (T)(1.0 / 3.0), (T)(1.0 / 6.0)};
         const T aw[3] = {(T)0.5, (T)0.5, (T)1.0};
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
-        for (int64_t k = nck - 1; k >= 0; --k) {
-            const int64_t len = std::min(every, adj_T - k * every);
-            plane_copy(*sg_psi[0], *ck_psi[k]);
-            if (res) plane_copy(*sg_n[0], *ck_n[k]);
-            for (int64_t j = 0; j < len; ++j) {
-                DevBuf* sp[3] = {st_psi[3 * j].get(), st_psi[3 * j + 1].get(), st_psi[3 * j + 2].get()};
-                DevBuf* sn[3] = {res ? st_n[3 * j].get() : nullptr, res ? st_n[3 * j + 1].get() : nullptr,
-                                 res ? st_n[3 * j + 2].get() : nullptr};
-                DevBuf& op = j + 1 < len ? *sg_psi[j + 1] : scratch_psi;
-                DevBuf* on = res ? (j + 1 < len ? sg_n[j + 1].get() : &scratch_n) : nullptr;
-                if (adj_fused)
-                    rk4_recompute_fused(*sg_psi[j], res ? sg_n[j].get() : nullptr, sp, sn, op, on);
-                else
-                    rk4_recompute(*sg_psi[j], res ? sg_n[j].get() : nullptr, sp, sn, op, on);
+        // Segment k's recompute (states and stage values) does not depend on the
+        // vector-Jacobian sweep of segment k + 1.  With the fused sweep the
+        // recomputes run on a second stream into the other of two plane sets,
+        // overlapped with the sweep of the segment before; events order a set's
+        // reuse after the sweep that read it.
+        const bool overlap = adj_fused;
+        struct Overlap {
+            cudaStream_t s2 = nullptr;
+            cudaEvent_t start = nullptr, rec_done[2] = {nullptr, nullptr}, vjp_done[2] = {nullptr, nullptr};
+            ~Overlap() {
+                if (s2) (void)cudaStreamSynchronize(s2);
+                for (cudaEvent_t e : {start, rec_done[0], rec_done[1], vjp_done[0], vjp_done[1]})
+                    if (e) (void)cudaEventDestroy(e);
+                if (s2) (void)cudaStreamDestroy(s2);
             }
+        } ov;
+        bool vjp_used[2] = {false, false};
+        if (overlap) {
+            PHX_CUDA(cudaStreamCreateWithFlags(&ov.s2, cudaStreamNonBlocking));
+            for (cudaEvent_t* e : {&ov.start, &ov.rec_done[0], &ov.rec_done[1], &ov.vjp_done[0], &ov.vjp_done[1]})
+                PHX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            PHX_CUDA(cudaEventRecord(ov.start, stream));
+            PHX_CUDA(cudaStreamWaitEvent(ov.s2, ov.start, 0));
+        }
+        auto recompute_segment = [&](int64_t k, int set) {
+            auto& SGp = set ? sg_psi2 : sg_psi;
+            auto& SGn = set ? sg_n2 : sg_n;
+            auto& STp = set ? st_psi2 : st_psi;
+            auto& STn = set ? st_n2 : st_n;
+            struct StreamSwap {  // the recompute's launches go to the second stream
+                cudaStream_t& a;
+                cudaStream_t& b;
+                bool on;
+                StreamSwap(cudaStream_t& x, cudaStream_t& y, bool o) : a(x), b(y), on(o) {
+                    if (on) std::swap(a, b);
+                }
+                ~StreamSwap() {
+                    if (on) std::swap(a, b);
+                }
+            };
+            if (overlap && vjp_used[set]) PHX_CUDA(cudaStreamWaitEvent(ov.s2, ov.vjp_done[set], 0));
+            StreamSwap sw(stream, ov.s2, overlap);
+            const int64_t len = std::min(every, adj_T - k * every);
+            plane_copy(*SGp[0], *ck_psi[k]);
+            if (res) plane_copy(*SGn[0], *ck_n[k]);
+            for (int64_t j = 0; j < len; ++j) {
+                DevBuf* sp[3] = {STp[3 * j].get(), STp[3 * j + 1].get(), STp[3 * j + 2].get()};
+                DevBuf* sn[3] = {res ? STn[3 * j].get() : nullptr, res ? STn[3 * j + 1].get() : nullptr,
+                                 res ? STn[3 * j + 2].get() : nullptr};
+                DevBuf& op = j + 1 < len ? *SGp[j + 1] : scratch_psi;
+                DevBuf* on = res ? (j + 1 < len ? SGn[j + 1].get() : &scratch_n) : nullptr;
+                if (adj_fused)
+                    rk4_recompute_fused(*SGp[j], res ? SGn[j].get() : nullptr, sp, sn, op, on);
+                else
+                    rk4_recompute(*SGp[j], res ? SGn[j].get() : nullptr, sp, sn, op, on);
+            }
+            if (overlap) PHX_CUDA(cudaEventRecord(ov.rec_done[set], stream));
+        };
+        if (overlap) recompute_segment(nck - 1, (int)((nck - 1) & 1));
+        for (int64_t k = nck - 1; k >= 0; --k) {
+            const int set = overlap ? (int)(k & 1) : 0;
+            if (overlap) {
+                if (k >= 1) recompute_segment(k - 1, set ^ 1);
+                PHX_CUDA(cudaStreamWaitEvent(stream, ov.rec_done[set], 0));
+            } else {
+                recompute_segment(k, 0);
+            }
+            auto& SGp = set ? sg_psi2 : sg_psi;
+            auto& SGn = set ? sg_n2 : sg_n;
+            auto& STp = set ? st_psi2 : st_psi;
+            auto& STn = set ? st_n2 : st_n;
+            const int64_t len = std::min(every, adj_T - k * every);
             for (int64_t j = len - 1; j >= 0; --j) {
                 if (adj_fused) {
                     AdjFusedParams<T> Q;
@@ -1917,11 +1983,11 @@ struct Engine final : EngineBase {
                     Q.N_r = N_r;
                     Q.N_c = N_c;
                     Q.pitch = pitch;
-                    Q.Ypsi[0] = cplane(*sg_psi[j]);
-                    Q.Yn[0] = res ? rplane(*sg_n[j]) : nullptr;
+                    Q.Ypsi[0] = cplane(*SGp[j]);
+                    Q.Yn[0] = res ? rplane(*SGn[j]) : nullptr;
                     for (int s = 2; s <= 4; ++s) {
-                        Q.Ypsi[s - 1] = cplane(*st_psi[3 * j + s - 2]);
-                        Q.Yn[s - 1] = res ? rplane(*st_n[3 * j + s - 2]) : nullptr;
+                        Q.Ypsi[s - 1] = cplane(*STp[3 * j + s - 2]);
+                        Q.Yn[s - 1] = res ? rplane(*STn[3 * j + s - 2]) : nullptr;
                     }
                     Q.lam_psi = cplane(lam_psi[cur]);
                     Q.lam_n = res ? rplane(lam_n[cur]) : nullptr;
@@ -1974,8 +2040,8 @@ struct Engine final : EngineBase {
                     Q.N_r = N_r;
                     Q.N_c = N_c;
                     Q.pitch = pitch;
-                    Q.Ypsi = s == 1 ? cplane(*sg_psi[j]) : cplane(*st_psi[3 * j + s - 2]);
-                    Q.Yn = res ? (s == 1 ? rplane(*sg_n[j]) : rplane(*st_n[3 * j + s - 2])) : nullptr;
+                    Q.Ypsi = s == 1 ? cplane(*SGp[j]) : cplane(*STp[3 * j + s - 2]);
+                    Q.Yn = res ? (s == 1 ? rplane(*SGn[j]) : rplane(*STn[3 * j + s - 2])) : nullptr;
                     Q.lam_psi = cplane(lam_psi[cur]);
                     Q.lam_n = res ? rplane(lam_n[cur]) : nullptr;
                     Q.ybar_in_psi = cplane(yb_psi[(s + 1) & 1]);
@@ -2015,6 +2081,10 @@ struct Engine final : EngineBase {
                     PHX_CUDA(cudaGetLastError());
                 }
                 cur ^= 1;
+            }
+            if (overlap) {
+                PHX_CUDA(cudaEventRecord(ov.vjp_done[set], stream));
+                vjp_used[set] = true;
             }
         }
         dt = saved_dt;
