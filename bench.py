@@ -452,7 +452,7 @@ def run_tetm(pb, torch, dev, n):
                 psi0 = (1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
                 s.set_field(f"psi_{comp}", psi0)
                 s.set_field(f"pump_{comp}", ring, 0)
-            s.run(12)
+            s.run(20)  # past the autotuner's rounds (4 x 4 candidates)
             us, info = _device_us(torch, s, dev, 20)
             key = f"tetm_{n}_f32_noise" if dw else f"tetm_{n}_f32_deterministic"
             out[key] = {"us_per_iteration": us, "grid_point_updates_per_s": 2 * n * n / (us * 1e-6),
@@ -590,7 +590,7 @@ def main():
             dist.barrier()
 
     # launch-shape autotuning (untimed, before the warm-up): the library times
-    # every candidate launch shape twice over its first iterations
+    # every candidate launch shape over its first iterations (four rounds)
     tune_iters = 0
     while tune_iters < 64:
         info = solver.run(1)

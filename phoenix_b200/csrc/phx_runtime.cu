@@ -123,6 +123,7 @@ struct Engine final : EngineBase {
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
+    static constexpr int kTuneRounds = 4;  // rounds over the candidates (the first untimed)
     static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
     static constexpr int kFusedShapes = 9;       // shapes 8-12: persistent TMA-fed variants
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + kFusedShapes];
@@ -1557,10 +1558,11 @@ struct Engine final : EngineBase {
         }
     }
 
-    // Launch-shape autotuning: the first 2 x (candidates) iterations of a
-    // handle run each candidate shape twice (results do not depend on the
-    // shape: every point is computed by the same operations); the second round
-    // is timed and the fastest shape is kept, and remembered for the process:
+    // Launch-shape autotuning: the first kTuneRounds x (candidates) iterations
+    // of a handle run the candidate shapes round-robin (results do not depend
+    // on the shape: every point is computed by the same operations); the first
+    // round warms up, the shortest of the later rounds' times ranks each shape,
+    // and the fastest shape is kept, and remembered for the process:
     // a later handle of the same configuration (grid, precision, boundaries,
     // inputs, iterator, device) starts with it.  PHX_TUNE_CACHE=0 turns the
     // memory off.
@@ -1587,7 +1589,7 @@ struct Engine final : EngineBase {
         PHX_CUDA(cudaEventRecord(tb, stream));
         tune_ev[tune_step % n_candidates()].push_back({ta, tb});
         ++tune_step;
-        if (tune_step < 2 * n_candidates()) return;
+        if (tune_step < kTuneRounds * n_candidates()) return;
         PHX_CUDA(cudaStreamSynchronize(stream));
         float best = 1e30f;
         int best_sh = kDefaultShape;

@@ -270,7 +270,7 @@ def test_tuned_shape_is_remembered_per_configuration(require_gpu, monkeypatch):
         with pb.Solver(sp) as s:
             s.set_field("psi_plus", np.zeros((n, n)))
             first = s.run(1).launch_shape
-            last = s.run(29).launch_shape
+            last = s.run(39).launch_shape
         return first, last
 
     tuned = first_shape(192)[1]
