@@ -277,9 +277,13 @@ PHX_API phx_status phx_get_field_device(phx_handle* h, int32_t field, int32_t gr
  * `checkpoint_every` iterations (<= 0: ceil(sqrt(iterations))).
  * phx_adjoint_backward takes dL/dpsi_T (and dL/dn_T, or NULL for zero) of
  * the final state and writes dL/dpsi_0, dL/dn_0 and dL/dP (pump group 0) --
- * each may be NULL -- by recomputing one checkpoint segment at a time.  All
- * arrays are contiguous N_r x N_c device arrays in the build precision; the
- * adjoint of a complex value u + iv is dL/du + i dL/dv. */
+ * each may be NULL -- by recomputing the checkpoint segments last to first.
+ * The recompute of the next segment runs on a second stream that the call
+ * creates, beside the current segment's gradient sweep, so two segments'
+ * states and stage values are held at once; the call returns after both
+ * streams' work is done.  All arrays are contiguous N_r x N_c device arrays in
+ * the build precision; the adjoint of a complex value u + iv is
+ * dL/du + i dL/dv. */
 PHX_API phx_status phx_adjoint_forward(phx_handle* h, int64_t iterations, int64_t checkpoint_every);
 PHX_API phx_status phx_adjoint_backward(phx_handle* h, const void* dpsi_T, const void* dn_T, void* dpsi_0, void* dn_0,
                                         void* dpump);
