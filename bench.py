@@ -460,6 +460,32 @@ def run_tetm(pb, torch, dev, n):
     return out
 
 
+def tetm_fp32_error(pb, dev, n=512, iters=200):
+    """FP32 error of the TE/TM configuration: rel-L2 of psi+ and psi- between
+    FP32 and FP64 runs from the same inputs (ring pump, delta_LT 0.05 meV,
+    g_pm = -0.2 g_c, no noise; dt scaled from 0.0015 ps at 4096^2 with dx^2)."""
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n, dtype=np.float64)
+    X, Y = np.meshgrid(x, x)
+    ring = 1.5 * P_TH * np.exp(-(np.sqrt(X ** 2 + Y ** 2) - 20.0) ** 2 / (2 * 3.0 ** 2))
+    rng = np.random.default_rng(4)
+    psi0 = {c: 1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) for c in ("plus", "minus")}
+    finals = {}
+    for dtype in ("f32", "f64"):
+        sp = pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                                 periodic_boundary_y=True, dtype=dtype, iterator="RK4", dt=0.0015 * (4096.0 / n) ** 2,
+                                 t0=0.0, t_max=1e12, fft_every=1e12, pump_temporal=[pb.Temporal()], device=dev,
+                                 use_twin_mode=True)
+        sp.g_pm, sp.delta_LT = -0.2 * PHYS["g_c"], 0.05
+        with pb.Solver(sp) as s:
+            for c in ("plus", "minus"):
+                s.set_field(f"psi_{c}", psi0[c])
+                s.set_field(f"pump_{c}", ring, 0)
+            s.run(iters)
+            finals[dtype] = {c: s.get_field(f"psi_{c}").astype(np.complex128) for c in ("plus", "minus")}
+    return {c: float(np.linalg.norm(finals["f32"][c] - finals["f64"][c]) / np.linalg.norm(finals["f64"][c]))
+            for c in ("plus", "minus")}
+
+
 def run_configs(pb, torch, device):
     """The other configurations: 256^2 FP64 RK4 (1000 steps); 1024^2 FP64 RK4,
     DP45 adaptive (rtol 1e-6) in FP32 and FP64 and the FP32-vs-FP64 error of
@@ -512,6 +538,7 @@ def run_configs(pb, torch, device):
                                                   "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt}
     # config 3: 4096^2 TE/TM FP32
     out.update(run_tetm(pb, torch, dev, 4096))
+    out["tetm_fp32_vs_fp64_rel_l2_512_after_200_rk4"] = tetm_fp32_error(pb, dev)
     return out
 
 
