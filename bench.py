@@ -416,6 +416,15 @@ def run_adjoint(pb, torch, device, iters=500, n=512):
                     "between the two"}
 
 
+def tune(solver, cap=600):
+    """Run single iterations until the library's launch-shape autotuning has
+    ended (launch_shape >= 0); returns the iterations run."""
+    for k in range(1, cap + 1):
+        if solver.run(1).launch_shape >= 0:
+            return k
+    raise RuntimeError("autotuning did not end")
+
+
 def _device_us(torch, solver, device, iters):
     """Device time per iteration of `iters` iterations (CUDA events on the solver stream)."""
     st = torch.cuda.ExternalStream(solver.stream, device=device)
@@ -452,7 +461,7 @@ def run_tetm(pb, torch, dev, n):
                 psi0 = (1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))).astype(np.complex64)
                 s.set_field(f"psi_{comp}", psi0)
                 s.set_field(f"pump_{comp}", ring, 0)
-            s.run(20)  # past the autotuner's rounds (4 x 4 candidates)
+            tune(s)
             us, info = _device_us(torch, s, dev, 20)
             key = f"tetm_{n}_f32_noise" if dw else f"tetm_{n}_f32_deterministic"
             out[key] = {"us_per_iteration": us, "grid_point_updates_per_s": 2 * n * n / (us * 1e-6),
@@ -507,7 +516,7 @@ def run_configs(pb, torch, device):
     with pb.Solver(sysp(n, "f64", dt=0.04)) as s:
         s.set_field("psi_plus", wl["psi0"])
         s.set_field("pump_plus", wl["pump"], 0)
-        s.run(40)
+        tune(s)
         us, info = _device_us(torch, s, dev, 1000)
         out["rk4_256_f64"] = {"us_per_iteration": us, "iterations": info.iterations, "launch_shape": info.launch_shape}
     # config 2: 1024^2 -- FP64 RK4, FP32 vs FP64, DP45 adaptive
@@ -519,7 +528,7 @@ def run_configs(pb, torch, device):
             s.set_field("psi_plus", wl["psi0"])
             s.set_field("pump_plus", wl["pump"], 0)
             s.set_field("potential_plus", wl["potential"], 0)
-            s.run(40)
+            tune(s)
             us, info = _device_us(torch, s, dev, 460)
             finals[dtype] = s.get_field("psi_plus").astype(np.complex128)
             out[f"rk4_1024_{dtype}"] = {"us_per_iteration": us, "launch_shape": info.launch_shape}
@@ -532,7 +541,7 @@ def run_configs(pb, torch, device):
             s.set_field("psi_plus", wl["psi0"])
             s.set_field("pump_plus", wl["pump"], 0)
             s.set_field("potential_plus", wl["potential"], 0)
-            s.run(20)
+            tune(s)
             us, info = _device_us(torch, s, dev, 100)
             out[f"dp45_adaptive_1024_{dtype}"] = {"us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
                                                   "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt}
@@ -617,13 +626,11 @@ def main():
             dist.barrier()
 
     # launch-shape autotuning (untimed, before the warm-up): the library times
-    # every candidate launch shape over its first iterations (four rounds)
-    tune_iters = 0
-    while tune_iters < 64:
-        info = solver.run(1)
-        tune_iters += 1
-        if info.launch_shape >= 0:
-            break
+    # every candidate launch shape over its first iterations (six rounds of
+    # three iterations each, medians, incumbent kept within 3 %)
+    tune_iters = tune(solver)
+    autotune = {"chosen": solver.run(0).launch_shape,
+                "median_us_per_iteration": {str(k): round(v, 3) for k, v in solver.tune_report().items()}}
 
     # warm-up
     for _ in range(args.warmup):
@@ -808,6 +815,7 @@ def main():
                              "step_alg_bytes": alg_pp * n * n,
                              "step_frac": alg_pp * n * n / (step_ms * 1e-3) / 1e9 / peak},
                 "kernel_avg_ms": kernels_ms, "launch_shape": shape, "autotune_iterations": tune_iters,
+                "autotune": autotune,
                 "gpu_launches": launches, "fft_filters_in_timed_region": filters,
                 "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu, "sweep": sweep,
                 "adjoint": adjoint, "configs": configs}

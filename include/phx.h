@@ -254,6 +254,13 @@ PHX_API phx_status phx_profile_enable(phx_handle* h, int32_t enable);
  * to or from HBM (each input and output plane touched once per point). */
 PHX_API phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes);
 
+/* Result of the launch-shape autotuning (no reference counterpart): the
+ * candidate shapes the handle timed and the median device time of one
+ * iteration with each, in microseconds (count = 0 before tuning has ended or
+ * when the configuration has no shape choice).  Up to `capacity` entries are
+ * written; *count receives the number available. */
+PHX_API phx_status phx_tune_read(phx_handle* h, int32_t capacity, int32_t* shapes, double* median_us, int32_t* count);
+
 /* The handle's cudaStream_t, as void*. */
 PHX_API phx_status phx_get_stream(phx_handle* h, void** stream);
 

@@ -77,6 +77,8 @@ _SIGS = {
     "phx_sum_abs2": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "phx_field_device_ptr": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     "phx_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "phx_tune_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                C.POINTER(C.c_int32)]),
     "phx_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
     "phx_profile_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_double)]),

@@ -24,6 +24,7 @@
 #include <array>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/phx.h"
@@ -50,6 +51,7 @@ struct EngineBase {
     std::string last_error;
     TemporalSpec pump_t[kMaxGroups], pot_t[kMaxGroups], pulse_t[kMaxGroups];
     bool force_fixed = false;  // phx_iterate(force_fixed_time_step): no step-size control this call
+    std::vector<std::pair<int, double>> tune_medians;  // (shape, median us per iteration) of the last tuning
     virtual ~EngineBase() = default;
     virtual void set_spectrum_output(bool enable) = 0;
     virtual void init() = 0;
@@ -123,7 +125,9 @@ struct Engine final : EngineBase {
     static constexpr int CPT = Pack<T>::CPT;
     int shape = -1;                 // launch shape in use (kShapeRB / kShapeWarps), -1 = tuning
     int tune_step = 0;              // steps run while tuning
-    static constexpr int kTuneRounds = 4;  // rounds over the candidates (the first untimed)
+    static constexpr int kTuneRounds = 6;  // rounds over the candidates (the first untimed)
+    static constexpr int kTuneIters = 3;   // consecutive iterations of one candidate per sample
+    static constexpr double kTuneMargin = 0.03;  // a challenger must beat the incumbent by this fraction
     static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
     static constexpr int kFusedShapes = 9;       // shapes 8-12: persistent TMA-fed variants
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + kFusedShapes];
@@ -230,6 +234,7 @@ struct Engine final : EngineBase {
             if (v >= 0 && v < kShapes) shape = v;
             if (v >= kFusedShape && v < kFusedShape + kFusedShapes && fused_eligible_static()) shape = v;
         }
+        if (shape < 0 && shape_free()) shape = kDefaultShape;
         if (shape < 0 && tune_cache_on()) {
             std::lock_guard<std::mutex> lk(tune_cache_mu());
             auto it = tune_cache().find(tune_key());
@@ -252,7 +257,20 @@ struct Engine final : EngineBase {
     int first_candidate() const { return fused_eligible_static() ? kFusedShape : 0; }
     int n_candidates() const { return fused_eligible_static() ? kFusedShapes : kShapes; }
     bool is_fused(int sh) const { return sh >= kFusedShape; }
-    int cur_shape() const { return shape >= 0 ? shape : first_candidate() + tune_step % n_candidates(); }
+    int cur_shape() const {
+        return shape >= 0 ? shape : first_candidate() + (tune_step / kTuneIters) % n_candidates();
+    }
+    // the shape kept unless a challenger is clearly faster: 64 x 16 tiles of
+    // the TMA iteration with two 12-warp CTAs per SM where the one-kernel
+    // iteration applies (fastest at 1024^2 and 4096^2 on B200), else the
+    // stage kernels' default
+    int incumbent() const { return fused_eligible_static() ? kFusedShape + 6 : kDefaultShape; }
+    // iterations whose kernels do not depend on the launch shape: no tuning
+    bool shape_free() const {
+        if (P.iterator == PHX_ITER_SSFM) return true;
+        if (P.iterator != PHX_ITER_RK4 || imag_time()) return false;
+        return (P.tetm && tetm_fused_on()) || (!P.tetm && !fused_eligible_static() && general_fused_on());
+    }
     // the fused iteration handles scalar RK4 with at most one pump and one
     // potential group and no pulse (real temporal coefficients are checked
     // every iteration)
@@ -1558,11 +1576,15 @@ struct Engine final : EngineBase {
         }
     }
 
-    // Launch-shape autotuning: the first kTuneRounds x (candidates) iterations
-    // of a handle run the candidate shapes round-robin (results do not depend
-    // on the shape: every point is computed by the same operations); the first
-    // round warms up, the shortest of the later rounds' times ranks each shape,
-    // and the fastest shape is kept, and remembered for the process:
+    // Launch-shape autotuning: the first kTuneRounds x kTuneIters x
+    // (candidates) iterations of a handle run the candidate shapes round-robin,
+    // kTuneIters consecutive iterations per candidate and round (results do not
+    // depend on the shape: every point is computed by the same operations).
+    // The first round warms up; each later round gives one sample per shape
+    // (the summed device time of its iterations), and the median sample ranks
+    // the shapes.  The incumbent shape is kept unless the fastest median beats
+    // it by more than kTuneMargin, so that boxes whose timings differ by noise
+    // pick the same shape.  The kept shape is remembered for the process:
     // a later handle of the same configuration (grid, precision, boundaries,
     // inputs, iterator, device) starts with it.  PHX_TUNE_CACHE=0 turns the
     // memory off.
@@ -1587,26 +1609,38 @@ struct Engine final : EngineBase {
     void tune_record(cudaEvent_t ta, cudaEvent_t tb) {
         tb = get_event();
         PHX_CUDA(cudaEventRecord(tb, stream));
-        tune_ev[tune_step % n_candidates()].push_back({ta, tb});
+        tune_ev[(tune_step / kTuneIters) % n_candidates()].push_back({ta, tb});
         ++tune_step;
-        if (tune_step < kTuneRounds * n_candidates()) return;
+        if (tune_step < kTuneRounds * kTuneIters * n_candidates()) return;
         PHX_CUDA(cudaStreamSynchronize(stream));
-        float best = 1e30f;
-        int best_sh = kDefaultShape;
+        double best = 1e300;
+        int best_sh = incumbent();
+        double inc_ms = 1e300;
+        tune_medians.clear();
         for (int sh = 0; sh < n_candidates(); ++sh) {
-            float ms = 1e30f;
-            for (size_t i = 1; i < tune_ev[sh].size(); ++i) {
-                float m = 0.f;
-                PHX_CUDA(cudaEventElapsedTime(&m, tune_ev[sh][i].first, tune_ev[sh][i].second));
-                ms = std::min(ms, m);
+            std::vector<double> samples;
+            for (int r = 1; r < kTuneRounds; ++r) {
+                double sum = 0.0;
+                for (int i = 0; i < kTuneIters; ++i) {
+                    const auto& pr = tune_ev[sh][(size_t)(r * kTuneIters + i)];
+                    float m = 0.f;
+                    PHX_CUDA(cudaEventElapsedTime(&m, pr.first, pr.second));
+                    sum += m;
+                }
+                samples.push_back(sum / kTuneIters);
             }
-            if (ms < best) best = ms, best_sh = first_candidate() + sh;
+            std::sort(samples.begin(), samples.end());
+            const double med = samples[samples.size() / 2];
+            tune_medians.push_back({first_candidate() + sh, med * 1e3});
+            if (med < best) best = med, best_sh = first_candidate() + sh;
+            if (first_candidate() + sh == incumbent()) inc_ms = med;
             for (auto& pr : tune_ev[sh]) {
                 event_pool.push_back(pr.first);
                 event_pool.push_back(pr.second);
             }
             tune_ev[sh].clear();
         }
+        if (inc_ms <= best * (1.0 + kTuneMargin)) best_sh = incumbent();
         shape = best_sh;
         if (tune_cache_on()) {
             std::lock_guard<std::mutex> lk(tune_cache_mu());
@@ -1766,7 +1800,8 @@ struct Engine final : EngineBase {
     }
     // The recompute's TMA iteration: the state planes change from one
     // iteration to the next; the launch's parameters carry their tensor maps.
-    std::map<std::pair<const void*, bool>, CUtensorMap> store_maps;
+    // (plane address, complex, box width, box height) -> encoded map
+    std::map<std::tuple<const void*, bool, int, int>, CUtensorMap> store_maps;
     template <bool RES, int TW, int TH, int NT, int MINB>
     void go_tma_store(const FusedParams<T>& F, DevBuf& yp, DevBuf* yn) {
         using Lay = TmaLayout<T, TW, TH>;
@@ -1779,15 +1814,15 @@ struct Engine final : EngineBase {
         }
         if (!err_flag.p) err_flag.alloc(sizeof(int), stream);
         if (!sm_count) PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
-        // a map depends only on the plane's address and on whether it is
-        // complex (pitch, rows and the boxes are fixed for this handle and
-        // this kernel), so encodings are kept per plane
+        // a map depends on the plane's address, on whether it is complex and
+        // on the box (the tile shape); pitch and rows are fixed for the handle
         auto map_of = [&](const void* base, bool complex, int box_h) -> const CUtensorMap& {
-            auto it = store_maps.find({base, complex});
+            const auto key = std::make_tuple(base, complex, TW + 8, box_h);
+            auto it = store_maps.find(key);
             if (it == store_maps.end()) {
                 CUtensorMap m;
                 tensor_map(&m, const_cast<void*>(base), complex, TW + 8, box_h);
-                it = store_maps.emplace(std::make_pair(base, complex), m).first;
+                it = store_maps.emplace(key, m).first;
             }
             return it->second;
         };
@@ -2392,6 +2427,19 @@ phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_ms, int64
         if (total_ms) *total_ms = h->eng->prof_ms[kind];
         if (launches) *launches = h->eng->prof_count[kind];
         if (bytes) *bytes = h->eng->prof_bytes[kind];
+    });
+}
+
+phx_status phx_tune_read(phx_handle* h, int32_t capacity, int32_t* shapes, double* median_us, int32_t* count) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    return guard(h, [&] {
+        if (!count || capacity < 0 || (capacity > 0 && (!shapes || !median_us))) phx::fail(PHX_ERR_INVALID_ARG, "bad arguments");
+        const auto& m = h->eng->tune_medians;
+        *count = (int32_t)m.size();
+        for (int32_t i = 0; i < std::min<int32_t>(capacity, (int32_t)m.size()); ++i) {
+            shapes[i] = m[(size_t)i].first;
+            median_us[i] = m[(size_t)i].second;
+        }
     });
 }
 

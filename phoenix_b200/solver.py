@@ -298,6 +298,14 @@ class Solver:
                 out[name] = {"ms": ms.value, "launches": n.value, "bytes": b.value}
         return out
 
+    def tune_report(self) -> Dict[int, float]:
+        """Launch shape -> median device microseconds per iteration, as timed
+        by the autotuner (empty before tuning has ended)."""
+        cap = 32
+        shapes, meds, n = (C.c_int32 * cap)(), (C.c_double * cap)(), C.c_int32()
+        L.check(self._lib.phx_tune_read(self._h, cap, shapes, meds, C.byref(n)), self._h)
+        return {int(shapes[i]): float(meds[i]) for i in range(min(cap, n.value))}
+
     @property
     def stream(self) -> int:
         s = C.c_void_p()

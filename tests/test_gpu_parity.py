@@ -248,7 +248,7 @@ def test_autotuning_across_every_shape_is_bit_identical(require_gpu, monkeypatch
             s.set_field("n_plus", np.zeros((n, n)))
             s.set_field("pump_plus", wl["pump"], 0)
             s.set_field("potential_plus", wl["potential"], 0)
-            info = s.run(40)
+            info = s.run(200)  # 9 candidates x 6 rounds x 3 iterations of tuning, then more
             if shape is None:
                 assert info.launch_shape >= 0  # tuning finished within the run
             outs.append((s.get_field("psi_plus"), s.get_field("n_plus")))
@@ -270,7 +270,7 @@ def test_tuned_shape_is_remembered_per_configuration(require_gpu, monkeypatch):
         with pb.Solver(sp) as s:
             s.set_field("psi_plus", np.zeros((n, n)))
             first = s.run(1).launch_shape
-            last = s.run(39).launch_shape
+            last = s.run(199).launch_shape
         return first, last
 
     tuned = first_shape(192)[1]
@@ -279,6 +279,30 @@ def test_tuned_shape_is_remembered_per_configuration(require_gpu, monkeypatch):
     assert first_shape(200)[0] == -1
     monkeypatch.setenv("PHX_TUNE_CACHE", "0")
     assert first_shape(192)[0] == -1
+
+
+def test_tuning_reports_medians_and_keeps_the_incumbent_within_margin(require_gpu, monkeypatch):
+    """The tuner reports a median time for every candidate shape; the shape it
+    keeps is the fastest one, or the incumbent (shape 10) when that is within
+    3 % of the fastest."""
+    import bench as B
+
+    monkeypatch.setenv("PHX_TUNE_CACHE", "0")
+    monkeypatch.delenv("PHX_STAGE_SHAPE", raising=False)
+    n = 512
+    sp = B.system(pb, n, "f32", 0)
+    sp.fft_every = 1e12
+    with pb.Solver(sp) as s:
+        s.set_field("psi_plus", np.zeros((n, n)))
+        assert s.tune_report() == {}
+        k = B.tune(s)
+        assert k == 9 * 6 * 3
+        rep = s.tune_report()
+        chosen = s.run(0).launch_shape
+    assert sorted(rep) == list(range(4, 13))
+    assert all(v > 0 for v in rep.values())
+    best = min(rep.values())
+    assert rep[chosen] == best or (chosen == 10 and rep[10] <= best * 1.03)
 
 
 def test_bad_field_shape_is_rejected(require_gpu):
