@@ -168,42 +168,82 @@ def write_txt(path, arr, digits=9):
             np.savetxt(f, np.imag(arr), fmt=f"%.{digits}g")
 
 
-def reference_cpu_run(n, dtype, iters, wl, gpu=False):
-    """Run the reference build for `iters` RK4 iterations of the workload and
-    return (us_per_iteration, cores, binary) or None.  CPU build: all host
-    cores.  GPU build (gpu=True): the reference's own CUDA code for sm_100 on
-    this GPU, one subgrid (the like-for-like bar for the kernels)."""
+def reference_binary(dtype, gpu):
+    """The reference build for a precision: its CUDA build for sm_100 (gpu), else
+    its CPU build (-march=x86-64-v3 when present)."""
     variant = "fp32" if dtype == "f32" else "fp64"
     if gpu:
         cand = [os.path.join(REF_BIN, f"phoenix_gpu_{variant}")]
     else:
         cand = [os.path.join(REF_BIN, f"phoenix_cpu_{variant}_v3"), os.path.join(REF_BIN, f"phoenix_cpu_{variant}")]
-    binary = next((b for b in cand if os.path.exists(b)), None)
+    return next((b for b in cand if os.path.exists(b)), None)
+
+
+_RUNTIME = re.compile(r"Total Runtime:\s*([0-9.eE+-]+)\s*s\s*-->.*?-->.*?-->\s*([0-9.eE+-]+)\s*mus/it")
+
+
+def reference_marginal(dtype, n, dt, t_lo, t_hi, loads=(), extra=(), gpu=False, fft_every=1e9, subgrids=None,
+                       phys=None):
+    """Marginal cost per iteration of the reference's main loop: the same run to
+    t_lo and to t_hi, (runtime_hi - runtime_lo) / (iterations_hi - iterations_lo)
+    from its `Total Runtime ... mus/it` line, so that set-up, the first
+    iterations and exit cancel.  loads: (flag, array, component) inputs written
+    as PHOENIX text matrices.  CPU build: every host core.  Returns a dict or
+    None when the build is missing or a run fails."""
+    binary = reference_binary(dtype, gpu)
     if binary is None:
         return None
     cores = os.cpu_count() or 1
+    ph = dict(PHYS, **(phys or {}))
+    runs = []
     with tempfile.TemporaryDirectory() as tmp:
-        files = {}
-        for key in ("psi0", "pump", "potential", "mask"):
-            files[key] = os.path.join(tmp, key + ".txt")
-            write_txt(files[key], wl[key])
-        dt = dt_for(n)
-        t_max = iters * dt * (1 - 1e-9)
-        args = [binary, "--N", str(n), str(n), "--L", str(L_BOX), str(L_BOX), "--dt", repr(dt), "--tmax", repr(t_max),
-                "--outEvery", "1e9", "--output", "none", "--path", os.path.join(tmp, "out"), "--threads", str(cores),
-                "--boundary", "periodic", "periodic", "--hbarscaled", str(PHYS["h_bar_s"]), "--meff",
-                str(PHYS["m_eff"]), "--gammaC", str(PHYS["gamma_c"]), "--gammaR", str(PHYS["gamma_r"]), "--gc",
-                str(PHYS["g_c"]), "--gr", str(PHYS["g_r"]), "--R", str(PHYS["R"]), "--fftEvery",
-                repr(MASK_EVERY * dt * (1 - 1e-6)), "--initState", "load", files["psi0"], "1", "add", "both",
-                "--pump", "load", files["pump"], "1", "add", "both", "--potential", "load", files["potential"], "1",
-                "add", "both", "--fftMask", "load", files["mask"], "1", "add", "both"]
-        if gpu:
-            args += ["--subgrids", "1", "1"]
-        proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
-        m = re.search(r"-->\s*([0-9.eE+-]+)\s*mus/it", proc.stdout)
-        if proc.returncode != 0 or not m:
-            return None
-        return float(m.group(1)), cores, os.path.basename(binary)
+        largs = []
+        for k, (flag, arr, comp) in enumerate(loads):
+            path = os.path.join(tmp, f"in{k}.txt")
+            write_txt(path, arr)
+            largs += [flag, "load", path, "1", "add", comp]
+        for t_max in (t_lo, t_hi):
+            args = [binary, "--N", str(n), str(n), "--L", str(L_BOX), str(L_BOX), "--dt", repr(dt),
+                    "--tmax", repr(t_max), "--outEvery", "1e9", "--output", "none", "--path",
+                    os.path.join(tmp, "out"), "--threads", str(cores), "--boundary", "periodic", "periodic",
+                    "--hbarscaled", str(ph["h_bar_s"]), "--meff", str(ph["m_eff"]), "--gammaC", str(ph["gamma_c"]),
+                    "--gammaR", str(ph["gamma_r"]), "--gc", str(ph["g_c"]), "--gr", str(ph["g_r"]), "--R",
+                    str(ph["R"]), "--fftEvery", repr(fft_every)] + largs + list(extra)
+            if subgrids:
+                args += ["--subgrids", str(subgrids), str(subgrids)]
+            proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
+            m = _RUNTIME.search(proc.stdout)
+            if proc.returncode != 0 or not m or float(m.group(2)) <= 0:
+                return None
+            total = float(m.group(1))
+            runs.append((total, round(total / float(m.group(2)) * 1e6)))
+    (s_lo, k_lo), (s_hi, k_hi) = runs
+    if k_hi <= k_lo:
+        return None
+    return {"us_per_iteration": (s_hi - s_lo) / (k_hi - k_lo) * 1e6, "iterations": [k_lo, k_hi],
+            "whole_run_us_per_iteration": s_hi / k_hi * 1e6, "cores": cores, "binary": os.path.basename(binary)}
+
+
+def scalar_loads(wl, mask=True, potential=True):
+    loads = [("--initState", wl["psi0"], "both"), ("--pump", wl["pump"], "both")]
+    if potential:
+        loads.append(("--potential", wl["potential"], "both"))
+    if mask:
+        loads.append(("--fftMask", wl["mask"], "both"))
+    return loads
+
+
+def reference_cpu_run(n, dtype, iters, wl):
+    """The reference CPU build on the 1024^2 workload (mask every 100
+    iterations): marginal microseconds per RK4 iteration over `iters`
+    iterations beyond the first 100, all host cores; (us, cores, what) or None."""
+    dt = dt_for(n)
+    r = reference_marginal(dtype, n, dt, 100 * dt * (1 - 1e-9), (100 + iters) * dt * (1 - 1e-9), scalar_loads(wl),
+                           fft_every=MASK_EVERY * dt * (1 - 1e-6))
+    if r is None:
+        return None
+    return r["us_per_iteration"], r["cores"], f"{r['binary']} (iterations {r['iterations'][0]} and " \
+                                              f"{r['iterations'][1]}, difference of the two runs)"
 
 
 def oracle_port_run(n, dtype, iters, wl):
@@ -225,7 +265,7 @@ def run_reference_arm(args):
         return 0
     n = args.n
     wl = workload(n)
-    iters = max(3, min(args.steps + args.warmup, args.ref_iters))
+    iters = max(100, min(args.steps + args.warmup, args.ref_iters))
     res = reference_cpu_run(n, args.dtype, iters, wl)
     kind = "reference"
     if res is None:
@@ -237,7 +277,8 @@ def run_reference_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
             "config": config_dict(args),
             "cpu_baseline": {"value": us, "unit": "us/iter", "cores": cores, "kind": kind,
-                             "sample": f"{iters} RK4 iterations of the {n}^2 workload with {what}"},
+                             "sample": f"{iters} RK4 iterations of the {n}^2 workload beyond its first 100 "
+                                       f"with {what}"},
             "e2e": {"value": us, "unit": "us/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -469,38 +510,40 @@ def run_tetm(pb, torch, dev, n):
     return out
 
 
-def tetm_fp32_error(pb, dev, n=512, iters=200):
-    """FP32 error of the TE/TM configuration: rel-L2 of psi+ and psi- between
-    FP32 and FP64 runs from the same inputs (ring pump, delta_LT 0.05 meV,
-    g_pm = -0.2 g_c, no noise; dt scaled from 0.0015 ps at 4096^2 with dx^2)."""
-    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n, dtype=np.float64)
-    X, Y = np.meshgrid(x, x)
-    ring = 1.5 * P_TH * np.exp(-(np.sqrt(X ** 2 + Y ** 2) - 20.0) ** 2 / (2 * 3.0 ** 2))
-    rng = np.random.default_rng(4)
-    psi0 = {c: 1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) for c in ("plus", "minus")}
-    finals = {}
-    for dtype in ("f32", "f64"):
-        sp = pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
-                                 periodic_boundary_y=True, dtype=dtype, iterator="RK4", dt=0.0015 * (4096.0 / n) ** 2,
-                                 t0=0.0, t_max=1e12, fft_every=1e12, pump_temporal=[pb.Temporal()], device=dev,
-                                 use_twin_mode=True)
-        sp.g_pm, sp.delta_LT = -0.2 * PHYS["g_c"], 0.05
-        with pb.Solver(sp) as s:
-            for c in ("plus", "minus"):
-                s.set_field(f"psi_{c}", psi0[c])
-                s.set_field(f"pump_{c}", ring, 0)
-            s.run(iters)
-            finals[dtype] = {c: s.get_field(f"psi_{c}").astype(np.complex128) for c in ("plus", "minus")}
-    return {c: float(np.linalg.norm(finals["f32"][c] - finals["f64"][c]) / np.linalg.norm(finals["f64"][c]))
-            for c in ("plus", "minus")}
+def run_dp45(pb, torch, dev, n, dtype, steps):
+    """Dormand-Prince 5(4) adaptive (tol 1e-6) on the n^2 workload: tuning, then
+    `steps` accepted steps timed on the device, with the library's per-kernel
+    times (the leg profiles run alone: `bench.py --only dp45 --steps 3`)."""
+    wl = workload(n)
+    sp = pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                             periodic_boundary_y=True, dtype=dtype, iterator="DP45", dt=dt_for(n), t0=0.0, t_max=1e12,
+                             fft_every=1e12, pump_temporal=[pb.Temporal()], potential_temporal=[pb.Temporal()],
+                             use_adaptive_timestep=True, tolerance=1e-6, dt_min=1e-5, dt_max=0.05, device=dev)
+    with pb.Solver(sp) as s:
+        s.set_field("psi_plus", wl["psi0"])
+        s.set_field("pump_plus", wl["pump"], 0)
+        s.set_field("potential_plus", wl["potential"], 0)
+        tune(s)
+        s.profile(True)
+        us, info = _device_us(torch, s, dev, steps)
+        kernels = {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
+                   for k, v in s.profile_read().items()}
+    return {"grid": n, "dtype": dtype, "us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
+            "accepted": info.accepted, "rejected": info.rejected, "kernels": kernels}
 
 
-def run_configs(pb, torch, device):
+def _ref_gpu(res):
+    return None if res is None else round(res["us_per_iteration"], 2)
+
+
+def run_configs(pb, torch, device, ref_gpu=True):
     """The other configurations: 256^2 FP64 RK4 (1000 steps); 1024^2 FP64 RK4,
-    DP45 adaptive (rtol 1e-6) in FP32 and FP64 and the FP32-vs-FP64 error of
-    RK4; 4096^2 TE/TM FP32 RK4 with a ring pump and noise (dw 1e-3) and its
-    deterministic twin.  Device time per iteration after the launch-shape
-    autotuning (40 untimed iterations)."""
+    DP45 adaptive (rtol 1e-6) in FP32 and FP64; 4096^2 TE/TM FP32 RK4 with a
+    ring pump and noise (dw 1e-3) and its deterministic twin.  Device time per
+    iteration after the launch-shape autotuning, each beside the reference's
+    own CUDA build on the same GPU with the same flags (reference_gpu_us,
+    marginal per iteration), and the FP32-vs-FP64 error of each configuration
+    at its own size and length (fp32_error)."""
     out = {}
     dev = device
 
@@ -510,6 +553,12 @@ def run_configs(pb, torch, device):
                                    periodic_boundary_y=True, dtype=dtype, iterator=it, dt=dt, t0=0.0, t_max=1e12,
                                    fft_every=1e12, pump_temporal=[pb.Temporal()], device=dev, **kw)
 
+    def rgpu(*a, **k):
+        if not ref_gpu:
+            return None
+        torch.cuda.synchronize()
+        return _ref_gpu(reference_marginal(*a, gpu=True, **k))
+
     # config 1: 256^2 FP64 RK4, dt 0.04, 1000 steps
     n = 256
     wl = workload(n, seed=1)
@@ -518,11 +567,13 @@ def run_configs(pb, torch, device):
         s.set_field("pump_plus", wl["pump"], 0)
         tune(s)
         us, info = _device_us(torch, s, dev, 1000)
-        out["rk4_256_f64"] = {"us_per_iteration": us, "iterations": info.iterations, "launch_shape": info.launch_shape}
-    # config 2: 1024^2 -- FP64 RK4, FP32 vs FP64, DP45 adaptive
+        out["rk4_256_f64"] = {"us_per_iteration": us, "iterations": info.iterations, "launch_shape": info.launch_shape,
+                              "reference_gpu_us": rgpu("f64", n, 0.04, 200 * 0.04 * (1 - 1e-9), 1200 * 0.04 * (1 - 1e-9),
+                                                       scalar_loads(wl, mask=False, potential=False), subgrids=1)}
+    # config 2: 1024^2 -- FP64 RK4, DP45 adaptive
     n = 1024
     wl = workload(n)
-    finals = {}
+    dt = dt_for(n)
     for dtype in ("f32", "f64"):
         with pb.Solver(sysp(n, dtype, potential_temporal=[pb.Temporal()])) as s:
             s.set_field("psi_plus", wl["psi0"])
@@ -530,10 +581,11 @@ def run_configs(pb, torch, device):
             s.set_field("potential_plus", wl["potential"], 0)
             tune(s)
             us, info = _device_us(torch, s, dev, 460)
-            finals[dtype] = s.get_field("psi_plus").astype(np.complex128)
-            out[f"rk4_1024_{dtype}"] = {"us_per_iteration": us, "launch_shape": info.launch_shape}
-    out["fp32_vs_fp64_rel_l2_after_500_rk4"] = float(np.linalg.norm(finals["f32"] - finals["f64"]) /
-                                                     np.linalg.norm(finals["f64"]))
+            out[f"rk4_1024_{dtype}"] = {
+                "us_per_iteration": us, "launch_shape": info.launch_shape,
+                "reference_gpu_us": rgpu(dtype, n, dt, 100 * dt * (1 - 1e-9), 600 * dt * (1 - 1e-9),
+                                         scalar_loads(wl, mask=False), subgrids=1)}
+    dp = ["-adaptive", "--iterator", "DP45", "--tol", "1e-06", "--rkvdt", "1e-05", "0.05"]
     for dtype in ("f32", "f64"):
         sp = sysp(n, dtype, it="DP45", potential_temporal=[pb.Temporal()], use_adaptive_timestep=True,
                   tolerance=1e-6, dt_min=1e-5, dt_max=0.05)
@@ -543,11 +595,92 @@ def run_configs(pb, torch, device):
             s.set_field("potential_plus", wl["potential"], 0)
             tune(s)
             us, info = _device_us(torch, s, dev, 100)
-            out[f"dp45_adaptive_1024_{dtype}"] = {"us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
-                                                  "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt}
+            out[f"dp45_adaptive_1024_{dtype}"] = {
+                "us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
+                "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt,
+                "reference_gpu_us": rgpu(dtype, n, dt, 0.2, 0.8, scalar_loads(wl, mask=False), extra=dp, subgrids=1)}
     # config 3: 4096^2 TE/TM FP32
     out.update(run_tetm(pb, torch, dev, 4096))
-    out["tetm_fp32_vs_fp64_rel_l2_512_after_200_rk4"] = tetm_fp32_error(pb, dev)
+    if ref_gpu:
+        dt3 = 0.0015
+        tetm = ["-tetm", "--gpm", repr(-0.2 * PHYS["g_c"]), "--deltaLT", "0.05", "--initRandom", "0.01", "4",
+                "--pump", repr(1.5 * P_TH), "add", "10", "10", "0", "0", "both", "1", "none", "gauss+noDivide"]
+        for key, dw in (("tetm_4096_f32_deterministic", "0"), ("tetm_4096_f32_noise", "0.001")):
+            out[key]["reference_gpu_us"] = rgpu("f32", 4096, dt3, 20 * dt3 * (1 - 1e-9), 70 * dt3 * (1 - 1e-9),
+                                                extra=tetm + ["--dw", dw], subgrids=16)
+    for k, v in out.items():
+        mine = v.get("us_per_iteration", v.get("us_per_accepted_step"))
+        if v.get("reference_gpu_us"):
+            v["speedup_vs_reference_gpu"] = v["reference_gpu_us"] / mine
+    out["fp32_error"] = fp32_errors(pb, dev)
+    return out
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, dtype=np.complex128), np.asarray(b, dtype=np.complex128)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def fp32_errors(pb, dev):
+    """FP32 against FP64 from identical inputs, rel-L2 of psi and n, per
+    configuration at its own size and length: config 1 (256^2, 1000 RK4
+    iterations), config 2 (1024^2 with disorder and the mask every 100
+    iterations: 5000 RK4 iterations; Dormand-Prince adaptive at tol 1e-6 to
+    t = 20 ps), config 3 (4096^2 TE/TM, 2000 RK4 iterations, deterministic),
+    config 5 (512^2, 500 RK4 iterations, the inverse-design pump disc)."""
+    out = {}
+
+    def run(sp, loads, iters=None):
+        res = {}
+        for dtype in ("f32", "f64"):
+            sp.dtype = dtype
+            with pb.Solver(sp) as s:
+                for name, arr, g in loads:
+                    s.set_field(name, arr, g)
+                info = s.run(iters) if iters else s.run()
+                res[dtype] = ({k: s.get_field(k) for k in ("psi_plus", "n_plus", "psi_minus", "n_minus")
+                               if k.endswith("plus") or sp.use_twin_mode}, info)
+        return {k: _rel(res["f32"][0][k], res["f64"][0][k]) for k in res["f64"][0]}, res
+
+    def base(n, dt, iterator="RK4", **kw):
+        return pb.SystemParameters(N_c=n, N_r=n, L_x=L_BOX, L_y=L_BOX, **PHYS, periodic_boundary_x=True,
+                                   periodic_boundary_y=True, dtype="f64", iterator=iterator, dt=dt, t0=0.0,
+                                   t_max=1e12, fft_every=1e12, pump_temporal=[pb.Temporal()], device=dev, **kw)
+
+    wl = workload(256, seed=1)
+    out["cfg1_rk4_256_1000"], _ = run(base(256, 0.04), [("psi_plus", wl["psi0"], 0), ("pump_plus", wl["pump"], 0)],
+                                      1000)
+    wl = workload(1024)
+    dt = dt_for(1024)
+    loads = [("psi_plus", wl["psi0"], 0), ("pump_plus", wl["pump"], 0), ("potential_plus", wl["potential"], 0),
+             ("fft_mask_plus", wl["mask"], 0)]
+    sp = base(1024, dt, potential_temporal=[pb.Temporal()])
+    sp.fft_every = MASK_EVERY * dt * (1 - 1e-6)
+    out["cfg2_rk4_1024_5000_mask"], _ = run(sp, loads, 5000)
+    sp = base(1024, dt, potential_temporal=[pb.Temporal()], iterator="DP45", use_adaptive_timestep=True,
+              tolerance=1e-6, dt_min=1e-5, dt_max=0.05)
+    sp.fft_every, sp.t_max = MASK_EVERY * dt * (1 - 1e-6), 20.0
+    err, res = run(sp, loads)
+    err["accepted_f32_f64"] = [res["f32"][1].accepted, res["f64"][1].accepted]
+    out["cfg2_dp45_1024_t20ps_mask"] = err
+    n = 4096
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n, dtype=np.float64)
+    X, Y = np.meshgrid(x, x)
+    ring = 1.5 * P_TH * np.exp(-(np.sqrt(X ** 2 + Y ** 2) - 20.0) ** 2 / (2 * 3.0 ** 2))
+    del X, Y
+    rng = np.random.default_rng(4)
+    psi = {c: 1e-2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) for c in ("plus", "minus")}
+    sp = base(n, 0.0015, use_twin_mode=True)
+    sp.g_pm, sp.delta_LT = -0.2 * PHYS["g_c"], 0.05
+    out["cfg3_tetm_4096_2000"], _ = run(sp, [("psi_plus", psi["plus"], 0), ("psi_minus", psi["minus"], 0),
+                                             ("pump_plus", ring, 0), ("pump_minus", ring, 0)], 2000)
+    del psi, ring
+    n = 512
+    x = -L_BOX / 2 + L_BOX / (n - 1) * np.arange(n)
+    X, Y = np.meshgrid(x, x)
+    disc = np.where(X ** 2 + Y ** 2 <= 30.0 ** 2, 1.2 * P_TH, 0.0)
+    psi0 = 1e-2 * (np.random.default_rng(6).standard_normal((n, n)) + 1j * np.random.default_rng(7).standard_normal((n, n)))
+    out["cfg5_rk4_512_500"], _ = run(base(n, 0.04), [("psi_plus", psi0, 0), ("pump_plus", disc, 0)], 500)
     return out
 
 
@@ -575,7 +708,8 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=200, help="timed iterations of the batched sweep")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (inverse-design) leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' timings")
-    ap.add_argument("--only", choices=["configs", "adjoint", "sweep", "tetm"], help="run one leg alone and print its JSON")
+    ap.add_argument("--only", choices=["configs", "adjoint", "sweep", "tetm", "dp45"],
+                    help="run one leg alone and print its JSON")
     ap.add_argument("--tetm-n", type=int, default=4096, help="grid of the --only tetm leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -594,7 +728,8 @@ def main():
         torch.cuda.set_device(0)
         leg = {"configs": lambda: run_configs(pb, torch, 0), "adjoint": lambda: run_adjoint(pb, torch, 0),
                "sweep": lambda: run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, 0),
-               "tetm": lambda: run_tetm(pb, torch, 0, args.tetm_n)}[args.only]
+               "tetm": lambda: run_tetm(pb, torch, 0, args.tetm_n),
+               "dp45": lambda: run_dp45(pb, torch, 0, args.n, args.dtype, args.steps)}[args.only]
         print(json.dumps({args.only: leg()}))
         return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -776,16 +911,20 @@ def main():
         us, cores, what = res
         cpu = {"value": us, "unit": "us/iter", "cores": cores, "kind": kind,
                "sample": f"{args.cpu_iters if kind == 'reference' else 3} RK4 iterations of the {n}^2 workload "
-                         f"with {what}"}
+                         f"(beyond its first 100 for the reference) with {what}"}
 
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         torch.cuda.synchronize()
-        res = reference_cpu_run(n, args.dtype, args.ref_gpu_iters, wl, gpu=True)
+        dt = dt_for(n)
+        res = reference_marginal(args.dtype, n, dt, 100 * dt * (1 - 1e-9), (100 + args.ref_gpu_iters) * dt * (1 - 1e-9),
+                                 scalar_loads(wl), gpu=True, fft_every=MASK_EVERY * dt * (1 - 1e-6), subgrids=1)
         if res is not None:
-            ref_gpu = {"value": res[0], "unit": "us/iter", "binary": res[2], "iterations": args.ref_gpu_iters,
-                       "note": "the reference's own CUDA build for sm_100 on this GPU, --subgrids 1 1, wall clock "
-                               "of its main loop (its mus/it line)"}
+            ref_gpu = {"value": res["us_per_iteration"], "unit": "us/iter", "binary": res["binary"],
+                       "iterations": res["iterations"],
+                       "note": "the reference's own CUDA build for sm_100 on this GPU, --subgrids 1 1: marginal wall "
+                               "clock of its main loop per iteration between the two runs (its Total Runtime / "
+                               "mus/it lines)"}
 
     sweep = None
     if rank == 0 and args.sweep_instances > 0:

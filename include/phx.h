@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define PHX_ABI_VERSION 2
+#define PHX_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define PHX_API __attribute__((visibility("default")))
@@ -47,7 +47,8 @@ typedef enum {
     PHX_ERR_NONFINITE = 4,    /* NaN or Inf found in a reduction            */
     PHX_ERR_TIMEOUT = 5,      /* a bounded wait gave up                     */
     PHX_ERR_UNSUPPORTED = 6,  /* valid request this build does not support  */
-    PHX_ERR_STATE = 7         /* call not valid in the handle's state       */
+    PHX_ERR_STATE = 7,        /* call not valid in the handle's state       */
+    PHX_ERR_ABORTED = 8       /* stopped by phx_request_abort               */
 } phx_status;
 
 typedef enum { PHX_F32 = 0, PHX_F64 = 1 } phx_dtype;
@@ -254,6 +255,23 @@ PHX_API phx_status phx_profile_enable(phx_handle* h, int32_t enable);
  * to or from HBM (each input and output plane touched once per point). */
 PHX_API phx_status phx_profile_read(phx_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes);
 
+/* Ask a running (or the next) phx_step / phx_iterate on this handle to stop
+ * before its next iteration; that call then returns PHX_ERR_ABORTED with
+ * its phx_step_info filled in and the state of the last completed iteration
+ * (no reference counterpart: the reference's main loop runs to t_max).  The
+ * one call that may come from another thread while the handle is in use;
+ * the request is consumed by the call it stops. */
+PHX_API phx_status phx_request_abort(phx_handle* h);
+
+/* Bound of the one-kernel RK4 iteration's wait for a tile's data (no
+ * reference counterpart): the number of polls of the tile's mbarrier before
+ * the wait gives up, also capped at about one second of device clock.  A wait
+ * that gives up makes the step return PHX_ERR_TIMEOUT; the iteration's result
+ * is then invalid, the handle stays usable.  polls < 0 restores the default
+ * (2^26); 0 makes every such wait give up at once, which exercises the error
+ * path without any fault. */
+PHX_API phx_status phx_set_wait_limit(phx_handle* h, int32_t polls);
+
 /* Result of the launch-shape autotuning (no reference counterpart): the
  * candidate shapes the handle timed and the median device time of one
  * iteration with each, in microseconds (count = 0 before tuning has ended or
@@ -283,8 +301,12 @@ PHX_API phx_status phx_get_field_device(phx_handle* h, int32_t field, int32_t gr
  * (as phx_step does) and keeps a checkpoint of the state every
  * `checkpoint_every` iterations (<= 0: ceil(sqrt(iterations))).
  * phx_adjoint_backward takes dL/dpsi_T (and dL/dn_T, or NULL for zero) of
- * the final state and writes dL/dpsi_0, dL/dn_0 and dL/dP (pump group 0) --
- * each may be NULL -- by recomputing the checkpoint segments last to first.
+ * the final state and writes dL/dpsi_0, dL/dn_0, dL/dP (pump group 0) and
+ * dL/dV (potential group 0) -- each may be NULL -- by recomputing the
+ * checkpoint segments last to first.  The pump and the potential enter the
+ * right-hand side as in gp_scalar (include/kernel/kernel_gp_compute.cuh:86-98):
+ * dL/dP through the reservoir's gain P c_P(t), dL/dV through
+ * (c_V(t) / hbar) V (-i psi).
  * The recompute of the next segment runs on a second stream that the call
  * creates, beside the current segment's gradient sweep, so two segments'
  * states and stage values are held at once; the call returns after both
@@ -293,7 +315,7 @@ PHX_API phx_status phx_get_field_device(phx_handle* h, int32_t field, int32_t gr
  * dL/du + i dL/dv. */
 PHX_API phx_status phx_adjoint_forward(phx_handle* h, int64_t iterations, int64_t checkpoint_every);
 PHX_API phx_status phx_adjoint_backward(phx_handle* h, const void* dpsi_T, const void* dn_T, void* dpsi_0, void* dn_0,
-                                        void* dpump);
+                                        void* dpump, void* dpotential);
 
 /* ---------------------------------------------------------------- batches
  * Many independent RK4 simulations -- pump-power sweeps, disorder

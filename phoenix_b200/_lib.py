@@ -16,7 +16,8 @@ HEADER = os.path.join(ROOT, "include", "phx.h")
 
 PHX_OK = 0
 STATUS = {0: "PHX_OK", 1: "PHX_ERR_INVALID_ARG", 2: "PHX_ERR_OOM", 3: "PHX_ERR_CUDA", 4: "PHX_ERR_NONFINITE",
-          5: "PHX_ERR_TIMEOUT", 6: "PHX_ERR_UNSUPPORTED", 7: "PHX_ERR_STATE"}
+          5: "PHX_ERR_TIMEOUT", 6: "PHX_ERR_UNSUPPORTED", 7: "PHX_ERR_STATE", 8: "PHX_ERR_ABORTED"}
+STATUS_CODES = {v: k for k, v in STATUS.items()}
 F32, F64 = 0, 1
 ITER = {"RK4": 0, "DP45": 1, "RK3": 2, "SSPRK3": 3, "MP": 4, "HEUN2": 5, "HEUN3": 6, "HW": 7, "NEWTON": 8,
         "NYSTROEM": 9, "RALSTON": 10, "RALSTON3": 11, "RALSTON4": 12, "RULE38": 13, "BOSHA": 14, "CASHKARP": 15,
@@ -28,7 +29,7 @@ FIELDS = {"psi_plus": 0, "psi_minus": 1, "n_plus": 2, "n_minus": 3, "pump_plus":
 COMPLEX_FIELDS = {"psi_plus", "psi_minus", "pulse_plus", "pulse_minus"}
 TEMPORAL = {"constant": 0, "iexp": 1, "osc": 1, "cos": 2, "gauss": 3}
 ENVELOPE = {"pump": 0, "potential": 1, "pulse": 2}
-ABI_VERSION = 2
+ABI_VERSION = 3
 KERNEL_KINDS = {"rk4_first": 0, "rk4_mid": 1, "rk4_last": 2, "stage": 3, "stage_final": 4, "stage_error": 5,
                 "filter": 6, "other": 7, "rk4_fused": 8}
 
@@ -77,6 +78,8 @@ _SIGS = {
     "phx_sum_abs2": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "phx_field_device_ptr": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     "phx_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "phx_request_abort": (C.c_int, [C.c_void_p]),
+    "phx_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int32]),
     "phx_tune_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int32)]),
     "phx_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -88,7 +91,8 @@ _SIGS = {
     "phx_set_field_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
     "phx_get_field_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64]),
     "phx_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64]),
-    "phx_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "phx_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
     "phx_batch_create": (C.c_int, [C.POINTER(Params), C.c_int32, C.POINTER(C.c_void_p)]),
     "phx_batch_destroy": (C.c_int, [C.c_void_p]),
     "phx_batch_set_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32]),

@@ -7,6 +7,9 @@
 //   kbar_4 = dt b4 lam',  kbar_s = dt b_s lam' + a_s dt Ybar_{s+1} (s = 3, 2, 1),
 //   Ybar_s = J_f(Y_s)^T kbar_s,  lam = lam' + Ybar_1 + ... + Ybar_4,
 //   Pbar  += sum_s c_s kbar_s^n               (dk_n / dP = c_s, the pump envelope)
+//   Vbar  += sum_s (c_V,s / hbar) Im(conj(kbar_s^psi) Y_s^psi)
+//                                  (dk_psi / dV = (c_V,s / hbar) (-i psi), the potential term
+//                                   of gp_scalar, kernel_gp_compute.cuh:93-98)
 // with a_1 = a_2 = 1/2, a_3 = 1.  One launch evaluates one stage s over the
 // interior; Ybar_{s+1} and lam' are read with a 5-point stencil because
 // J^T contains the (symmetric) Laplacian.
@@ -46,6 +49,7 @@ struct AdjParams {
     const T* pot;    // potential plane or nullptr
     const T* pump;   // pump plane or nullptr (only its presence matters: dP accumulates)
     T* pbar;         // dL/dP accumulator (interior), or nullptr
+    T* vbar;         // dL/dV accumulator (interior), or nullptr
     T c_pot, c_pump; // envelope coefficients of this stage
     T dt_b, a_dt;    // dt b_s and a_s dt (0 for s == 4)
     T A, ohb, ohb_gc, ohb_gr, half_R, half_gamma_c, gamma_r, R;
@@ -128,6 +132,7 @@ __global__ void __launch_bounds__(256) adj_stage_kernel(const __grid_constant__ 
     T gn = (T)0;
     if (Q.res) gn = Q.ohb_gr * im_mbar_psi + Q.half_R * re_mbar_psi - (Q.gamma_r + Q.R * norm) * m;
     if (Q.pbar) Q.pbar[i] += Q.c_pump * m;
+    if (Q.vbar) Q.vbar[i] += Q.ohb * Q.c_pot * im_mbar_psi;
     // lam = lam' + Ybar_4 + Ybar_3 + Ybar_2 + Ybar_1
     cx<T> acc;
     T accn = (T)0;
@@ -195,6 +200,7 @@ struct AdjFusedParams {
     T* out_n;
     const T* pot;
     T* pbar;
+    T* vbar;               // dL/dV accumulator, or nullptr
     T c_pot[4], c_pump[4];
     T dt_b[4], a_dt[4];    // dt b_s; a_s dt (a_4 unused)
     T A, ohb, ohb_gc, ohb_gr, half_R, half_gamma_c, gamma_r, R;
@@ -232,11 +238,11 @@ __global__ void __launch_bounds__(NT, MINB) adj_fused_kernel(const __grid_consta
         sL[k] = (r < Q.N_r + 4 && c < Q.N_c + 4) ? Q.lam_psi[(long long)r * p + c] : mk((T)0, (T)0);
     }
     __syncthreads();
-    T ybn[OWN], accn[OWN], pb[OWN];
+    T ybn[OWN], accn[OWN], pb[OWN], vb[OWN];
     cx<T> acc[OWN];
 #pragma unroll
     for (int j = 0; j < OWN; ++j) {
-        ybn[j] = (T)0, accn[j] = (T)0, pb[j] = (T)0;
+        ybn[j] = (T)0, accn[j] = (T)0, pb[j] = (T)0, vb[j] = (T)0;
         acc[j] = mk((T)0, (T)0);
     }
 #pragma unroll
@@ -332,6 +338,7 @@ __global__ void __launch_bounds__(NT, MINB) adj_fused_kernel(const __grid_consta
                 acc[j].im += g.im;
                 accn[j] += gn;
                 pb[j] += Q.c_pump[s - 1] * m;
+                if (Q.vbar) vb[j] += Q.ohb * Q.c_pot[s - 1] * im_mbar_psi;
             }
         }
         __syncthreads();
@@ -351,6 +358,7 @@ __global__ void __launch_bounds__(NT, MINB) adj_fused_kernel(const __grid_consta
         l.im += acc[j].im;
         Q.out_psi[i] = l;
         adj_images4(Q.N_r, Q.N_c, p, Q.out_psi, r, c, l);
+        if (Q.vbar) Q.vbar[i] += vb[j];
         if (Q.res) {
             const T ln = Q.lam_n[i] + accn[j];
             Q.out_n[i] = ln;

@@ -24,6 +24,7 @@
 #include <array>
 #include <map>
 #include <mutex>
+#include <atomic>
 #include <tuple>
 #include <vector>
 
@@ -52,6 +53,9 @@ struct EngineBase {
     TemporalSpec pump_t[kMaxGroups], pot_t[kMaxGroups], pulse_t[kMaxGroups];
     bool force_fixed = false;  // phx_iterate(force_fixed_time_step): no step-size control this call
     std::vector<std::pair<int, double>> tune_medians;  // (shape, median us per iteration) of the last tuning
+    // set by phx_request_abort (any thread); phx_step stops before its next iteration
+    std::atomic<int> abort_requested{0};
+    int wait_polls = kWaitPolls;  // bound of the TMA iteration's wait for a tile's data (phx_set_wait_limit)
     virtual ~EngineBase() = default;
     virtual void set_spectrum_output(bool enable) = 0;
     virtual void init() = 0;
@@ -64,7 +68,7 @@ struct EngineBase {
     virtual void field_ptr(int field, int group, void** ptr, int64_t* pitch) = 0;
     virtual void field_device(int field, int group, void* dev, int64_t count, bool upload) = 0;
     virtual void adjoint_forward(int64_t iterations, int64_t every) = 0;
-    virtual void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump) = 0;
+    virtual void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump, void* dpot) = 0;
 
     // ---- per-launch event timing (phx_profile_*)
     bool profiling = false;
@@ -739,6 +743,7 @@ struct Engine final : EngineBase {
         Q.has_pot = F.pot != nullptr;
         Q.tiles_x = (N_c + TW - 1) / TW;
         Q.err = static_cast<int*>(err_flag.p);
+        Q.wait_polls = wait_polls;
         if (!sm_count) PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
     }
     template <bool RES, int TW, int TH, int NT, int MINB = 1>
@@ -1293,6 +1298,11 @@ struct Engine final : EngineBase {
                 r7_cur = r[2];
             }
             accept = adapt_time_step(err, nrm);
+            // a non-finite error norm is rejected with dt * 0.9 (solver.cu:90-97);
+            // once dt is at dt_min no smaller step is left to try
+            if (!accept && !(std::isfinite(err) && std::isfinite(nrm)) && dt <= (T)P.dt_min)
+                fail(PHX_ERR_NONFINITE, "the adaptive error norm is not finite at the smallest step size dt_min "
+                                        "(NaN or Inf in the state)");
             if (accept) {
                 swap_state_with(sol_slot());
                 r7_prev = r7_cur;
@@ -1520,8 +1530,13 @@ struct Engine final : EngineBase {
         const int64_t l0 = launches;
         int64_t its = 0, acc = 0, rej = 0, filt = 0;
         const T t_max = (T)P.t_max, fft_every = (T)P.fft_every;
+        bool aborted = false;
         while (its < max_iterations) {
             if (t >= t_max) break;
+            if (abort_requested.exchange(0)) {
+                aborted = true;
+                break;
+            }
             if (P.stochastic_amplitude > 0.0) noise_amp = (T)P.stochastic_amplitude * std::sqrt(dt);
             update_kernel_time();
             t = t + dt;
@@ -1574,6 +1589,9 @@ struct Engine final : EngineBase {
             info->launch_shape = shape;
             info->reserved = 0;
         }
+        if (aborted)
+            fail(PHX_ERR_ABORTED, "stopped by phx_request_abort after " + std::to_string(its) +
+                                      " iterations; the state is that of the last completed iteration");
     }
 
     // Launch-shape autotuning: the first kTuneRounds x kTuneIters x
@@ -1685,7 +1703,7 @@ struct Engine final : EngineBase {
     std::vector<std::unique_ptr<DevBuf>> sg_psi, sg_n;    // states of one segment
     std::vector<std::unique_ptr<DevBuf>> st_psi, st_n;    // Y2..Y4 of every iteration of a segment
     std::vector<std::unique_ptr<DevBuf>> sg_psi2, sg_n2, st_psi2, st_n2;  // the second set (overlapped recompute)
-    DevBuf lam_psi[2], lam_n[2], yb_psi[2], yb_n[2], la_psi, la_n, pbar;
+    DevBuf lam_psi[2], lam_n[2], yb_psi[2], yb_n[2], la_psi, la_n, pbar, vbar;
     int64_t adj_T = 0, adj_every = 0;
     T adj_dt = 0;
     bool adj_ready = false;
@@ -1838,6 +1856,7 @@ struct Engine final : EngineBase {
         Q.tiles_x = (N_c + TW - 1) / TW;
         Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
         Q.err = static_cast<int*>(err_flag.p);
+        Q.wait_polls = wait_polls;
         const int blocks = std::min(Q.n_tiles, blocks_per_sm * sm_count);
         kern<<<blocks, NT, Lay::total, stream>>>(Q);
     }
@@ -1890,7 +1909,7 @@ struct Engine final : EngineBase {
         ++launches;
         PHX_CUDA(cudaGetLastError());
     }
-    void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump) override {
+    void adjoint_backward(const void* dpsi, const void* dn, void* dpsi0, void* dn0, void* dpump, void* dpot) override {
         if (!adj_ready) fail(PHX_ERR_STATE, "phx_adjoint_forward must run first");
         if (!dpsi) fail(PHX_ERR_INVALID_ARG, "dL/dpsi_T is NULL");
         adjoint_check();
@@ -1921,6 +1940,12 @@ struct Engine final : EngineBase {
         if (res && !la_n.p) la_n.alloc(rb, stream);
         if (!pbar.p) pbar.alloc(rb, stream);
         PHX_CUDA(cudaMemsetAsync(pbar.p, 0, rb, stream));
+        if (dpot && !P.n_potential_groups) fail(PHX_ERR_INVALID_ARG, "dL/dV needs a potential group");
+        const bool want_v = dpot != nullptr;
+        if (want_v) {
+            if (!vbar.p) vbar.alloc(rb, stream);
+            PHX_CUDA(cudaMemsetAsync(vbar.p, 0, rb, stream));
+        }
         // lam_T = dL/d(psi_T, n_T), with periodic images
         int cur = 0;
         unpack_interior_kernel<C><<<256, 256, 0, stream>>>(static_cast<const C*>(dpsi), cplane(lam_psi[0]), pitch, N_r, N_c);
@@ -2032,6 +2057,7 @@ struct Engine final : EngineBase {
                     Q.out_n = res ? rplane(lam_n[cur ^ 1]) : nullptr;
                     Q.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
                     Q.pbar = (res && P.n_pump_groups) ? rplane(pbar) : nullptr;
+                    Q.vbar = want_v ? rplane(vbar) : nullptr;
                     for (int s = 1; s <= 4; ++s) {
                         Q.c_pot[s - 1] = P.n_potential_groups ? interp<T>(amp_pot[0], next_pot[0], cw[s - 1]).real() : (T)0;
                         Q.c_pump[s - 1] = P.n_pump_groups ? interp<T>(amp_pump[0], next_pump[0], cw[s - 1]).real() : (T)0;
@@ -2092,6 +2118,7 @@ struct Engine final : EngineBase {
                     Q.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
                     Q.pump = P.n_pump_groups ? rplane(pump[0]) : nullptr;
                     Q.pbar = (res && P.n_pump_groups) ? rplane(pbar) : nullptr;
+                    Q.vbar = want_v ? rplane(vbar) : nullptr;
                     Q.c_pot = P.n_potential_groups ? interp<T>(amp_pot[0], next_pot[0], cw[s - 1]).real() : (T)0;
                     Q.c_pump = P.n_pump_groups ? interp<T>(amp_pump[0], next_pump[0], cw[s - 1]).real() : (T)0;
                     Q.dt_b = adj_dt * bw[s - 1];
@@ -2131,6 +2158,7 @@ struct Engine final : EngineBase {
             if (!(res && P.n_pump_groups)) fail(PHX_ERR_INVALID_ARG, "dL/dP needs a pump group and the reservoir");
             pack_interior_kernel<T><<<256, 256, 0, stream>>>(rplane(pbar), pitch, N_r, N_c, static_cast<T*>(dpump));
         }
+        if (want_v) pack_interior_kernel<T><<<256, 256, 0, stream>>>(rplane(vbar), pitch, N_r, N_c, static_cast<T*>(dpot));
         PHX_CUDA(cudaGetLastError());
         PHX_CUDA(cudaStreamSynchronize(stream));  // scratch planes are freed on return
         check_err_flag();
@@ -2153,7 +2181,9 @@ struct Engine final : EngineBase {
         PHX_CUDA(cudaGetLastError());
         PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
         PHX_CUDA(cudaStreamSynchronize(stream));
-        return static_cast<const double*>(host_result.p)[0];
+        const double v = static_cast<const double*>(host_result.p)[0];
+        if (!std::isfinite(v)) fail(PHX_ERR_NONFINITE, "the sum of |field|^2 is not finite: the field holds NaN or Inf");
+        return v;
     }
 };
 
@@ -2406,9 +2436,9 @@ phx_status phx_adjoint_forward(phx_handle* h, int64_t iterations, int64_t checkp
 }
 
 phx_status phx_adjoint_backward(phx_handle* h, const void* dpsi_T, const void* dn_T, void* dpsi_0, void* dn_0,
-                                void* dpump) {
+                                void* dpump, void* dpotential) {
     if (!h) return PHX_ERR_INVALID_ARG;
-    return guard(h, [&] { h->eng->adjoint_backward(dpsi_T, dn_T, dpsi_0, dn_0, dpump); });
+    return guard(h, [&] { h->eng->adjoint_backward(dpsi_T, dn_T, dpsi_0, dn_0, dpump, dpotential); });
 }
 
 phx_status phx_profile_enable(phx_handle* h, int32_t enable) {
@@ -2443,6 +2473,18 @@ phx_status phx_tune_read(phx_handle* h, int32_t capacity, int32_t* shapes, doubl
     });
 }
 
+phx_status phx_request_abort(phx_handle* h) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    h->eng->abort_requested.store(1);
+    return PHX_OK;
+}
+
+phx_status phx_set_wait_limit(phx_handle* h, int32_t polls) {
+    if (!h) return PHX_ERR_INVALID_ARG;
+    h->eng->wait_polls = polls < 0 ? phx::kWaitPolls : polls;
+    return PHX_OK;
+}
+
 phx_status phx_get_stream(phx_handle* h, void** stream) {
     if (!h || !stream) return PHX_ERR_INVALID_ARG;
     *stream = (void*)h->eng->stream;
@@ -2461,6 +2503,7 @@ const char* phx_status_string(int32_t s) {
         case PHX_ERR_OOM: return "out of memory";
         case PHX_ERR_CUDA: return "CUDA error";
         case PHX_ERR_NONFINITE: return "non-finite value";
+        case PHX_ERR_ABORTED: return "aborted on request";
         case PHX_ERR_TIMEOUT: return "timeout";
         case PHX_ERR_UNSUPPORTED: return "unsupported";
         case PHX_ERR_STATE: return "invalid state";

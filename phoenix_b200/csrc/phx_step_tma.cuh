@@ -40,7 +40,12 @@ struct TmaParams {
     int has_pump, has_pot;
     int tiles_x, n_tiles;
     int* err;              // set to 1 when a bounded wait gave up
+    int wait_polls;        // polls of a tile's mbarrier before the wait gives up (0: at once)
 };
+
+// polls of an mbarrier before a bounded wait gives up (also capped at ~1 s of
+// device clock)
+constexpr int kWaitPolls = 1 << 26;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -61,10 +66,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
         : "memory");
     return ok != 0;
 }
-// bounded wait: gives up after ~1 s of device clock
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+// bounded wait: gives up after max_polls polls or ~1 s of device clock
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int max_polls = kWaitPolls) {
     const long long t0 = clock64();
-    for (int it = 0; it < (1 << 26); ++it) {
+    for (int it = 0; it < max_polls; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if (clock64() - t0 > 2000000000LL) break;
     }
@@ -147,8 +152,12 @@ struct TileRef {
 // tensor maps and parameters live in global memory (one set per instance);
 // the maps are acquired for the tensor-map proxy before use and the tile's
 // parameters are staged in shared memory.
+// wait_polls bounds the wait for each tile's boxes (the error path gives up
+// there); the drain of loads still in flight after a failed wait always uses
+// the full bound, so no bulk copy lands in the shared memory of a CTA that
+// has left.
 template <typename T, bool RES, int TW, int TH, int NT, bool BATCH, bool STORE, typename TileOf>
-__device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles, int* err) {
+__device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles, int* err, int wait_polls) {
     using Lay = TmaLayout<T, TW, TH>;
     constexpr int W4 = Lay::W4, WR = Lay::WR;
     constexpr int W3 = TW + 6, H3 = TH + 6;
@@ -216,7 +225,7 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
         // thread 0 waits for the tile's boxes; the others wait at the barrier
         // (no issue slots spent spinning), which also orders the data thread 0
         // observed before their reads
-        const bool ok = threadIdx.x == 0 ? mbar_wait_bounded(&bars[slot], parity) : true;
+        const bool ok = threadIdx.x == 0 ? mbar_wait_bounded(&bars[slot], parity, wait_polls) : true;
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicExch(err, 1);
@@ -352,7 +361,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_tma_kernel(const __grid_constant
         R.tx0 = (g % Q.tiles_x) * TW;
         return R;
     };
-    tma_tile_loop<T, RES, TW, TH, NT, false, STORE>(tile_of, Q.n_tiles, Q.err);
+    tma_tile_loop<T, RES, TW, TH, NT, false, STORE>(tile_of, Q.n_tiles, Q.err, Q.wait_polls);
 }
 
 // ---------------------------------------------------------------- batches
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_batch_kernel(const __grid_consta
         R.tx0 = (local % I.tiles_x) * TW;
         return R;
     };
-    tma_tile_loop<T, RES, TW, TH, NT, true, false>(tile_of, B.n_tiles, B.err);
+    tma_tile_loop<T, RES, TW, TH, NT, true, false>(tile_of, B.n_tiles, B.err, kWaitPolls);
 }
 
 }  // namespace phx

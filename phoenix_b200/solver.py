@@ -230,8 +230,9 @@ class Solver:
         L.check(self._lib.phx_adjoint_forward(self._h, C.c_int64(iterations), C.c_int64(checkpoint_every)), self._h)
         self._order_torch_after()
 
-    def adjoint_backward(self, dpsi_T, dn_T=None, want_psi0=True, want_n0=True, want_pump=True):
-        """dL/d(final state) -> (dL/dpsi_0, dL/dn_0, dL/dP) as torch CUDA tensors (None where not wanted)."""
+    def adjoint_backward(self, dpsi_T, dn_T=None, want_psi0=True, want_n0=True, want_pump=True, want_potential=False):
+        """dL/d(final state) -> (dL/dpsi_0, dL/dn_0, dL/dP, dL/dV) as torch CUDA
+        tensors (None where not wanted; dL/dV needs a potential group)."""
         import torch
 
         f32 = self.system.dtype not in ("f64", "fp64", "double")
@@ -243,12 +244,13 @@ class Solver:
         g_psi = torch.empty(self._shape(), dtype=cdt, device=dev) if want_psi0 else None
         g_n = torch.empty(self._shape(), dtype=rdt, device=dev) if want_n0 and self.system.use_reservoir else None
         g_p = torch.empty(self._shape(), dtype=rdt, device=dev) if want_pump else None
+        g_v = torch.empty(self._shape(), dtype=rdt, device=dev) if want_potential else None
         ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
         self._order_after_torch()
-        L.check(self._lib.phx_adjoint_backward(self._h, ptr(dpsi_T), ptr(dn_T), ptr(g_psi), ptr(g_n), ptr(g_p)),
-                self._h)
+        L.check(self._lib.phx_adjoint_backward(self._h, ptr(dpsi_T), ptr(dn_T), ptr(g_psi), ptr(g_n), ptr(g_p),
+                                               ptr(g_v)), self._h)
         self._order_torch_after()
-        return g_psi, g_n, g_p
+        return g_psi, g_n, g_p, g_v
 
     # -- time
     @property
@@ -297,6 +299,16 @@ class Solver:
             if n.value:
                 out[name] = {"ms": ms.value, "launches": n.value, "bytes": b.value}
         return out
+
+    def request_abort(self):
+        """Ask a phx_step running in another thread to stop before its next
+        iteration (it then raises PhxError with PHX_ERR_ABORTED)."""
+        L.check(self._lib.phx_request_abort(self._h), self._h)
+
+    def set_wait_limit(self, polls: int):
+        """Bound of the one-kernel iteration's wait for a tile's data, in polls
+        (< 0: the default; 0: every such wait gives up at once)."""
+        L.check(self._lib.phx_set_wait_limit(self._h, int(polls)), self._h)
 
     def tune_report(self) -> Dict[int, float]:
         """Launch shape -> median device microseconds per iteration, as timed

