@@ -187,7 +187,8 @@ def reference_marginal(dtype, n, dt, t_lo, t_hi, loads=(), extra=(), gpu=False, 
     """Marginal cost per iteration of the reference's main loop: the same run to
     t_lo and to t_hi, (runtime_hi - runtime_lo) / (iterations_hi - iterations_lo)
     from its `Total Runtime ... mus/it` line, so that set-up, the first
-    iterations and exit cancel.  loads: (flag, array, component) inputs written
+    iterations and exit cancel.  An untimed run to t_lo goes first, so that
+    neither timed run is the first on a cold device or page cache.  loads: (flag, array, component) inputs written
     as PHOENIX text matrices.  CPU build: every host core.  Returns a dict or
     None when the build is missing or a run fails."""
     binary = reference_binary(dtype, gpu)
@@ -202,7 +203,7 @@ def reference_marginal(dtype, n, dt, t_lo, t_hi, loads=(), extra=(), gpu=False, 
             path = os.path.join(tmp, f"in{k}.txt")
             write_txt(path, arr)
             largs += [flag, "load", path, "1", "add", comp]
-        for t_max in (t_lo, t_hi):
+        for t_max in (t_lo, t_lo, t_hi):
             args = [binary, "--N", str(n), str(n), "--L", str(L_BOX), str(L_BOX), "--dt", repr(dt),
                     "--tmax", repr(t_max), "--outEvery", "1e9", "--output", "none", "--path",
                     os.path.join(tmp, "out"), "--threads", str(cores), "--boundary", "periodic", "periodic",
@@ -217,7 +218,7 @@ def reference_marginal(dtype, n, dt, t_lo, t_hi, loads=(), extra=(), gpu=False, 
                 return None
             total = float(m.group(1))
             runs.append((total, round(total / float(m.group(2)) * 1e6)))
-    (s_lo, k_lo), (s_hi, k_hi) = runs
+    (s_lo, k_lo), (s_hi, k_hi) = runs[1], runs[2]
     if k_hi <= k_lo:
         return None
     return {"us_per_iteration": (s_hi - s_lo) / (k_hi - k_lo) * 1e6, "iterations": [k_lo, k_hi],
@@ -457,6 +458,14 @@ def run_adjoint(pb, torch, device, iters=500, n=512):
                     "between the two"}
 
 
+def flush_l2(buf):
+    """Evict L2 before a timed iteration: write a buffer twice the size of L2,
+    then read it, so that L2 holds clean lines of the buffer (the write-back of
+    the flush's own dirty lines is not charged to the timed iteration)."""
+    buf.zero_()
+    buf.view(-1, 4096).amax(dim=1)
+
+
 def tune(solver, cap=600):
     """Run single iterations until the library's launch-shape autotuning has
     ended (launch_shape >= 0); returns the iterations run."""
@@ -625,15 +634,16 @@ def fp32_errors(pb, dev):
     """FP32 against FP64 from identical inputs, rel-L2 of psi and n, per
     configuration at its own size and length: config 1 (256^2, 1000 RK4
     iterations), config 2 (1024^2 with disorder and the mask every 100
-    iterations: 5000 RK4 iterations; Dormand-Prince adaptive at tol 1e-6 to
-    t = 20 ps), config 3 (4096^2 TE/TM, 2000 RK4 iterations, deterministic),
+    iterations: 5000 RK4 iterations, bit-exact and fused multiply-add FP32;
+    Dormand-Prince adaptive at tol 1e-6 to t = 20 ps), config 3 (4096^2 TE/TM, 2000 RK4 iterations, deterministic),
     config 5 (512^2, 500 RK4 iterations, the inverse-design pump disc)."""
     out = {}
 
-    def run(sp, loads, iters=None):
+    def run(sp, loads, iters=None, fma=False):
         res = {}
         for dtype in ("f32", "f64"):
             sp.dtype = dtype
+            sp.fma = fma and dtype == "f32"
             with pb.Solver(sp) as s:
                 for name, arr, g in loads:
                     s.set_field(name, arr, g)
@@ -657,6 +667,7 @@ def fp32_errors(pb, dev):
     sp = base(1024, dt, potential_temporal=[pb.Temporal()])
     sp.fft_every = MASK_EVERY * dt * (1 - 1e-6)
     out["cfg2_rk4_1024_5000_mask"], _ = run(sp, loads, 5000)
+    out["cfg2_rk4_1024_5000_mask_fma"], _ = run(sp, loads, 5000, fma=True)
     sp = base(1024, dt, potential_temporal=[pb.Temporal()], iterator="DP45", use_adaptive_timestep=True,
               tolerance=1e-6, dt_min=1e-5, dt_max=0.05)
     sp.fft_every, sp.t_max = MASK_EVERY * dt * (1 - 1e-6), 20.0
@@ -689,7 +700,10 @@ def config_dict(args):
             "grid": [args.n, args.n], "iterator": "RK4", "boundary": "periodic", "dt_ps": dt_for(args.n),
             "mask_every_iterations": MASK_EVERY, "physics": "polariton GP + reservoir, meV/ps/um, hbar 0.6582, "
             "m_eff 5.6e-4 m_e", "replicas": "one independent simulation per GPU",
-            "l2": "256 MiB write between timed iterations (value); e2e runs back to back"}
+            "l2": "256 MiB write then read between timed iterations (value); e2e runs back to back",
+            "arithmetic": "every operation rounded separately in the reference's order (bit-identical to its FP32 "
+                          "/ FP64 build)" if args.arith == "exact" else
+                          "fused multiply-adds (phx_params.fma; FP32 error vs FP64 in configs.fp32_error)"}
 
 
 def main():
@@ -700,6 +714,9 @@ def main():
     ap.add_argument("--impl", default="phx", choices=["phx", "reference"])
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--arith", default="exact", choices=["exact", "fma"],
+                    help="arithmetic of the timed solver: exact (every operation rounded as the reference does) or "
+                         "fma (phx_params.fma, FP32)")
     ap.add_argument("--ref-iters", type=int, default=400, help="cap on reference CPU iterations")
     ap.add_argument("--cpu-iters", type=int, default=1500, help="CPU-baseline sample in the phx arm (about 10 s)")
     ap.add_argument("--ref-gpu-iters", type=int, default=500, help="iterations of the reference GPU build")
@@ -747,6 +764,7 @@ def main():
     n = args.n
     wl = workload(n)
     sp = system(pb, n, args.dtype, local)
+    sp.fma = args.arith == "fma"
     solver = pb.Solver(sp)
     solver.set_field("psi_plus", wl["psi0"])
     solver.set_field("n_plus", np.zeros((n, n)))
@@ -770,7 +788,7 @@ def main():
     # warm-up
     for _ in range(args.warmup):
         with torch.cuda.stream(stream):
-            flush.zero_()
+            flush_l2(flush)
         solver.run(1)
     torch.cuda.synchronize()
     barrier()
@@ -790,7 +808,7 @@ def main():
         # iterations ahead of the GPU, so that no event pair spans host time
         torch.cuda._sleep(50_000_000)
         for i in range(args.steps):
-            flush.zero_()
+            flush_l2(flush)
             starts[i].record(stream)
             info = solver.run(1)
             ends[i].record(stream)
@@ -816,6 +834,45 @@ def main():
     torch.cuda.synchronize()
     warm_ms = e0.elapsed_time(e1) / args.steps
     solver.close()
+
+    # the same workload with the fused multiply-add arithmetic (phx_params.fma),
+    # timed the same way (L2 flushed before every iteration)
+    sp_fma = system(pb, n, args.dtype, local)
+    sp_fma.fma = args.dtype == "f32" and args.arith == "exact"
+    fma_leg = None
+    if sp_fma.fma:
+        sf = pb.Solver(sp_fma)
+        sf.set_field("psi_plus", wl["psi0"])
+        sf.set_field("n_plus", np.zeros((n, n)))
+        sf.set_field("pump_plus", wl["pump"], 0)
+        sf.set_field("potential_plus", wl["potential"], 0)
+        sf.set_field("fft_mask_plus", wl["mask"])
+        tune(sf)
+        fstream = torch.cuda.ExternalStream(sf.stream, device=local)
+        for _ in range(args.warmup):
+            with torch.cuda.stream(fstream):
+                flush_l2(flush)
+            sf.run(1)
+        torch.cuda.synchronize()
+        fs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        fe = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        sf.profile(True)
+        with torch.cuda.stream(fstream):
+            torch.cuda._sleep(50_000_000)
+            for i in range(args.steps):
+                flush_l2(flush)
+                fs[i].record(fstream)
+                finfo = sf.run(1)
+                fe[i].record(fstream)
+            torch.cuda.synchronize()
+        fprof = sf.profile_read()
+        sf.close()
+        f_ms = sum(a.elapsed_time(b) for a, b in zip(fs, fe)) / args.steps
+        fk = fprof.get("rk4_fused")
+        fma_leg = {"value": f_ms * 1e3, "unit": "us/iter", "launch_shape": finfo.launch_shape,
+                   "kernel_avg_ms": fk["ms"] / fk["launches"] if fk else None,
+                   "note": "phx_params.fma = 1: the one-kernel iteration with fused multiply-adds (FP32), same "
+                           "workload and timing; its FP32-vs-FP64 error is in configs.fp32_error"}
 
     # end to end through the public API, host buffers in and out
     e2e_iters = args.steps
@@ -954,7 +1011,7 @@ def main():
                              "step_alg_bytes": alg_pp * n * n,
                              "step_frac": alg_pp * n * n / (step_ms * 1e-3) / 1e9 / peak},
                 "kernel_avg_ms": kernels_ms, "launch_shape": shape, "autotune_iterations": tune_iters,
-                "autotune": autotune,
+                "autotune": autotune, "fma": fma_leg,
                 "gpu_launches": launches, "fft_filters_in_timed_region": filters,
                 "clocks": clocks.summary(), "cpu_baseline": cpu, "reference_gpu": ref_gpu, "sweep": sweep,
                 "adjoint": adjoint, "configs": configs}

@@ -149,6 +149,13 @@ typedef struct {
                                        sum |f|^2 dV = A after each iteration); 0 = real time.
                                        Runge-Kutta iterators need use_reservoir = 0 (the complex
                                        step makes the reservoir complex); SSFM takes both */
+    int32_t fma;                    /* 1: the one-kernel scalar RK4 iteration (and the batch) evaluates
+                                       the right-hand side and the stage sums with fused multiply-adds,
+                                       regrouped (FP32 only; no reference counterpart).  About 40 %
+                                       fewer instructions per point; results then differ from the
+                                       reference FP32 build in the last bits (their FP32-vs-FP64
+                                       error is of the same size).  0: every operation rounded
+                                       separately in the reference's order (bit-identical). */
 } phx_params;
 
 typedef struct {
@@ -241,7 +248,8 @@ typedef enum {
     PHX_KERNEL_FILTER = 6,      /* k-space filter passes (without cuFFT)     */
     PHX_KERNEL_OTHER = 7,       /* rings, reductions                         */
     PHX_KERNEL_RK4_FUSED = 8,   /* whole RK4 iteration in one launch         */
-    PHX_KERNEL_KINDS = 9
+    PHX_KERNEL_DP45_FUSED = 9,  /* whole DP45 attempt in one launch          */
+    PHX_KERNEL_KINDS = 10
 } phx_kernel_kind;
 
 /* Per-launch CUDA-event timing of this handle's kernels (no reference

@@ -31,7 +31,7 @@ TEMPORAL = {"constant": 0, "iexp": 1, "osc": 1, "cos": 2, "gauss": 3}
 ENVELOPE = {"pump": 0, "potential": 1, "pulse": 2}
 ABI_VERSION = 3
 KERNEL_KINDS = {"rk4_first": 0, "rk4_mid": 1, "rk4_last": 2, "stage": 3, "stage_final": 4, "stage_error": 5,
-                "filter": 6, "other": 7, "rk4_fused": 8}
+                "filter": 6, "other": 7, "rk4_fused": 8, "dp45_fused": 9}
 
 
 class PhxError(RuntimeError):
@@ -50,7 +50,7 @@ class Params(C.Structure):
         ("dt", C.c_double), ("t0", C.c_double), ("t_max", C.c_double), ("tol", C.c_double), ("dt_min", C.c_double),
         ("dt_max", C.c_double), ("fft_every", C.c_double), ("stochastic_amplitude", C.c_double), ("seed", C.c_uint64),
         ("n_pump_groups", C.c_int32), ("n_potential_groups", C.c_int32), ("n_pulse_groups", C.c_int32),
-        ("device", C.c_int32), ("imag_time_amplitude", C.c_double),
+        ("device", C.c_int32), ("imag_time_amplitude", C.c_double), ("fma", C.c_int32),
     ]
 
 

@@ -80,6 +80,7 @@ struct BatchEngine final : BatchBase {
     };
     std::vector<std::unique_ptr<Instance>> inst;
     bool res = true;
+    bool fma = false;  // fused multiply-add arithmetic (phx_params.fma)
     int cur = 0;  // which ping-pong plane holds every instance's state
 
     // per tile shape: instance table and tile -> instance map on the device
@@ -117,6 +118,7 @@ struct BatchEngine final : BatchBase {
     void init(const phx_params* ps, int n) {
         device = ps[0].device;
         res = ps[0].use_reservoir != 0;
+        fma = ps[0].fma != 0;
         PHX_CUDA(cudaSetDevice(device));
         PHX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
@@ -192,6 +194,20 @@ struct BatchEngine final : BatchBase {
             }
         }
     }
+    // the kernel of shape S for this batch (reservoir or not, bit-exact or
+    // fused multiply-add arithmetic)
+    template <int S>
+    auto kernel_of() const {
+        using K = void (*)(BatchParams<T>);
+        K k = res ? (K)rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]>
+                  : (K)rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]>;
+        if constexpr (sizeof(T) == 4) {
+            if (fma)
+                k = res ? (K)rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S], true>
+                        : (K)rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S], true>;
+        }
+        return k;
+    }
     template <int S>
     void build_one() {
         std::vector<BatchInstance<T>> hi;
@@ -204,8 +220,7 @@ struct BatchEngine final : BatchBase {
         PHX_CUDA(cudaMemcpyAsync(d_inst[S].p, hi.data(), sizeof(BatchInstance<T>) * hi.size(), cudaMemcpyHostToDevice, stream));
         PHX_CUDA(cudaMemcpyAsync(d_tile[S].p, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice, stream));
         PHX_CUDA(cudaStreamSynchronize(stream));  // host vectors die here
-        auto kern = res ? rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]>
-                        : rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]>;
+        auto kern = kernel_of<S>();
         const int smem = TmaLayout<T, SH::TW[S], SH::TH[S]>::total;
         PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         int per_sm = 0;
@@ -232,10 +247,7 @@ struct BatchEngine final : BatchBase {
         B.dir = dir;
         B.err = static_cast<int*>(err_flag.p);
         const int smem = TmaLayout<T, SH::TW[S], SH::TH[S]>::total;
-        if (res)
-            rk4_batch_kernel<T, true, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]><<<blocks[S], SH::NT[S], smem, stream>>>(B);
-        else
-            rk4_batch_kernel<T, false, SH::TW[S], SH::TH[S], SH::NT[S], SH::MINB[S]><<<blocks[S], SH::NT[S], smem, stream>>>(B);
+        kernel_of<S>()<<<blocks[S], SH::NT[S], smem, stream>>>(B);
     }
     void launch(int sh, int dir) {
         switch (sh) {
@@ -477,6 +489,8 @@ void validate_batch(const phx_params* ps, int n) {
         if (p.N_c < 8 || p.N_r < 8) fail(PHX_ERR_INVALID_ARG, at + "grid must be at least 8 x 8");
         if ((long long)p.N_c * p.N_r > (1LL << 28)) fail(PHX_ERR_INVALID_ARG, at + "grid too large for a batch instance");
         if (p.dtype != ps[0].dtype) fail(PHX_ERR_INVALID_ARG, at + "all instances share one dtype");
+        if (p.fma != ps[0].fma) fail(PHX_ERR_INVALID_ARG, at + "all instances share one arithmetic (fma)");
+        if (p.fma && p.dtype != PHX_F32) fail(PHX_ERR_UNSUPPORTED, at + "the fused multiply-add arithmetic is FP32 only");
         if (p.dtype != PHX_F32 && p.dtype != PHX_F64) fail(PHX_ERR_INVALID_ARG, at + "dtype must be PHX_F32 or PHX_F64");
         if (p.dtype == PHX_F32 && (p.N_c & 1)) fail(PHX_ERR_UNSUPPORTED, at + "FP32 grids need an even N_c");
         if (p.use_reservoir != ps[0].use_reservoir) fail(PHX_ERR_INVALID_ARG, at + "all instances share use_reservoir");

@@ -1,0 +1,353 @@
+// One launch per Dormand-Prince 5(4) attempt (DormandPrince45::step with
+// variable dt, source/cuda_solver/solver/iterator/dormand_prince.cu:37-95):
+// the six stages k1..k6 with their sums, the solution Y7 = y0 + dt sum b_j k_j,
+// k7 = f(Y7), the error sum dt sum e_j k_j (runge_sum_to_error,
+// include/kernel/kernel_summation.cuh:270-289) and its FP64 reductions, on an
+// on-chip tile.
+//
+// The reference pads a subgrid by the halo H = 7 and lets stage s shrink the
+// evaluated region to the subgrid + (7 - s) cells (CALCULATE_K,
+// include/cuda/cuda_macro.cuh:110-134).  This kernel does the same around a
+// TW x TH output tile: the state is read once over tile + 7 into a shared
+// stencil buffer, stage s is evaluated over tile + (7 - s), the stage inputs
+// Y_s ping-pong between two shared buffers, every k_j is kept in shared memory
+// over the region where stage j evaluates it (tile + (7 - j)),
+// and y0, n0, pump and potential of the points a thread owns stay in its
+// registers.  Each point is computed with the operations, and in the order, of
+// the k-stack stage kernels (stage_scalar_kernel, kinds kStack / kStackError),
+// so the solution is bit-identical to theirs; only the FP64 error and norm
+// sums are added in another order.  HBM traffic per attempt drops from the
+// k-stack's 7 planes in and out per stage to the state in and the solution
+// out.
+//
+// Reference-norm rings (PHX_NORM_REFERENCE): the reference's error norm runs
+// over its halo-padded buffer, where ring rho = 1..6 holds the stages computed
+// that far out (error terms of k_1..k_{7-rho}, state Y_{8-rho}).  A tile whose
+// extended regions cover ring cells evaluates exactly those stages there (from
+// periodic images or from the zero ring, as the reference does), so it adds a
+// ring cell's terms at the stage 7 - rho that last reaches it, counting each
+// ring cell in the tile that holds the cell's nearest grid point.  Ring 7 (the
+// previous accepted state) is summed by ring7_kernel.
+#pragma once
+
+#include "phx_stage.cuh"
+#include "phx_step_fused.cuh"
+
+namespace phx {
+
+constexpr int kDpH = 7;   // halo of DP45 (k_max)
+constexpr int kDpImg = 7; // depth of the periodic images the kernel writes for its solution
+
+template <typename T>
+struct Dp45Params {
+    int N_r, N_c;
+    int img_x, img_y;   // periodic axes
+    long long pitch;
+    const cx<T>* psi0;  // state (interior origin, padded plane with >= 7-deep images / zero ring)
+    const T* n0;
+    cx<T>* psi1;        // solution Y7 (another plane), with 7-deep periodic images
+    T* n1;
+    const T* pump;      // one plane or nullptr
+    const T* pot;
+    T pump_c[7], pot_c[7];  // real temporal coefficients of stages 1..7
+    T m2, odx2, ody2, meff, ohb;
+    T ohb_gc, half_gamma_c, ohb_gr, half_R, gamma_r, R;
+    T w[6][6];  // weights of the sum forming Y_{s+1} after stage s (row s - 1); row 5 is b
+    T dtw1;     // dt * a_21, the single-weight sum of stage 1
+    T dt;
+    T e[7];     // error weights
+    int ring;   // add the reference-norm rings 1..6
+    double* partials;  // per block (error, norm)
+};
+
+template <typename T, int TW, int TH>
+struct Dp45Layout {
+    static constexpr int W6 = TW + 12, H6 = TH + 12;  // stage-1 region (tile + 6)
+    static constexpr int W7 = TW + 14, H7 = TH + 14;  // stencil input of stage 1 (tile + 7)
+    static constexpr int SW = W7 + 2;                 // padded row: pairs start on 16-byte boundaries
+    static constexpr int al(int b) { return (b + 127) / 128 * 128; }
+    // k_j (j = 1..5) over tile + (7 - j), i.e. rows j - 1 .. H6 - j of the
+    // stage-1 region, each row the full width W6 (so that a point pair is one
+    // aligned 16-byte access); k_j's row r (stage-1 coordinates) at
+    // kbase(j) + (r - (j - 1)) * W6.  k6 (psi only) likewise, TH + 2 rows.
+    __host__ __device__ static constexpr int kbase(int j) { return W6 * ((j - 1) * H6 - (j - 1) * (j - 2)); }
+    static constexpr int kpts = kbase(6) + (TH + 2) * W6;
+    static constexpr int knpts = kbase(6);  // k_n: j = 1..5
+    static constexpr int y_bytes = H7 * SW * 2 * (int)sizeof(T);
+    static constexpr int y0_off = 0;
+    static constexpr int y1_off = al(y_bytes);
+    static constexpr int yn_off = y1_off + al(y_bytes);
+    static constexpr int kp_off = yn_off + al(W6 * H6 * (int)sizeof(T));
+    static constexpr int kn_off = kp_off + al(kpts * 2 * (int)sizeof(T));
+    static constexpr int total = kn_off + al(knpts * (int)sizeof(T)) + 128;
+};
+
+// a pair of real values at an even index of a shared array (8 / 16 bytes)
+template <typename T>
+__device__ __forceinline__ void ld_rpair(const T* p, T& a, T& b) {
+    if constexpr (sizeof(T) == 4) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        a = v.x, b = v.y;
+    } else {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        a = v.x, b = v.y;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void st_rpair(T* p, T a, T b) {
+    if constexpr (sizeof(T) == 4)
+        *reinterpret_cast<float2*>(p) = make_float2(a, b);
+    else
+        *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
+// MINB: CTAs per SM the register allocation must leave room for
+template <typename T, bool RES, int TW, int TH, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_constant__ Dp45Params<T> P) {
+    static_assert(TW % 2 == 0, "pairs");
+    using Lay = Dp45Layout<T, TW, TH>;
+    constexpr int W6 = Lay::W6, H6 = Lay::H6, W7 = Lay::W7, H7 = Lay::H7, SW = Lay::SW;
+    static_assert(W6 % 2 == 0 && SW % 2 == 0, "aligned pairs");
+    constexpr int PW = W6 / 2;
+    constexpr int NP = PW * H6;
+    constexpr int OWN = (NP + NT - 1) / NT;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((128u - ((unsigned)__cvta_generic_to_shared(smem_raw) & 127u)) & 127u);
+    cx<T>* const sY0 = reinterpret_cast<cx<T>*>(smem + Lay::y0_off);
+    cx<T>* const sY1 = reinterpret_cast<cx<T>*>(smem + Lay::y1_off);
+    T* sYn = reinterpret_cast<T*>(smem + Lay::yn_off);
+    cx<T>* sK = reinterpret_cast<cx<T>*>(smem + Lay::kp_off);
+    T* sKn = reinterpret_cast<T*>(smem + Lay::kn_off);
+
+    const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
+    const long long pitch = P.pitch;
+    const bool has_pump = P.pump != nullptr, has_pot = P.pot != nullptr;
+    // loads stay inside the padded planes (ring 8); cells they clamp feed no
+    // value the reference computes (the argument of rk4_fused_kernel)
+    const int rmax = P.N_r + kRing - 1, cmax = P.N_c + kRing - 1;
+    // only tiles at the grid's border hold reference-norm ring cells
+    const bool ring_tile = P.ring && (tx0 == 0 || ty0 == 0 || tx0 + TW >= P.N_c || ty0 + TH >= P.N_r);
+
+    // 1) psi0 over tile + 7 into sY0: point (ry, rx) at ry * SW + rx + 1
+    for (int i = threadIdx.x; i < H7 * W7; i += NT) {
+        const int ry = i / W7, rx = i - ry * W7;
+        const int gy = min(ty0 - 7 + ry, rmax), gx = min(tx0 - 7 + rx, cmax);
+        sY0[ry * SW + rx + 1] = P.psi0[(long long)gy * pitch + gx];
+    }
+    // 2) pointwise values of the owned pairs (stage-1 region coordinates)
+    cx<T> y0[OWN][2];
+    T n0[OWN][2], pu[OWN][2], po[OWN][2];
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        const int p = threadIdx.x + NT * j;
+        const int qy = p / PW, qx = 2 * (p - qy * PW);
+        const bool own = p < NP;
+        const int gy = min(ty0 - 6 + qy, rmax);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int gx = min(tx0 - 6 + qx + h, cmax);
+            const long long g = (long long)gy * pitch + gx;
+            n0[j][h] = (RES && own) ? __ldg(P.n0 + g) : (T)0;
+            pu[j][h] = (RES && has_pump && own) ? __ldg(P.pump + g) : (T)0;
+            po[j][h] = (has_pot && own) ? __ldg(P.pot + g) : (T)0;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        const int p = threadIdx.x + NT * j;
+        const int qy = p / PW, qx = 2 * (p - qy * PW);
+        if (p < NP)
+            lds_pair(sY0 + (qy + 1) * SW + qx + 2, y0[j][0], y0[j][1]);
+        else
+            y0[j][0] = y0[j][1] = mk((T)0, (T)0);
+    }
+
+    double err_acc = 0.0, nrm_acc = 0.0;
+    // 3) stages 1..6; stage s covers margin s - 1 of the stage-1 region.  A
+    // pair straddling the region's x edge computes both points; the outer one
+    // is stored but never read as a value the reference computes.
+#pragma unroll 1
+    for (int s = 1; s <= 6; ++s) {
+        const int m = s - 1;
+        const cx<T>* in = (s & 1) ? sY0 : sY1;  // Y_s: stage 1 reads the state in sY0
+        cx<T>* out = (s & 1) ? sY1 : sY0;
+        const int ks = Lay::kbase(s) - m * W6;  // k_s row qy at ks + qy * W6
+#pragma unroll
+        for (int j = 0; j < OWN; ++j) {
+            const int p = threadIdx.x + NT * j;
+            const int qy = p / PW, qx = 2 * (p - qy * PW);
+            if (p >= NP || qy < m || qy >= H6 - m || qx + 1 < m || qx >= W6 - m) continue;
+            const int e = (qy + 1) * SW + qx + 2;  // stencil buffer index of the pair (even)
+            const int pi = qy * W6 + qx;           // stage-1 region index of the pair (even)
+            cx<T> c0, c1, u0, u1, d0, d1;
+            if (s == 1) {
+                c0 = y0[j][0], c1 = y0[j][1];
+            } else {
+                lds_pair(in + e, c0, c1);
+            }
+            lds_pair(in + e - SW, u0, u1);
+            lds_pair(in + e + SW, d0, d1);
+            const cx<T> lft = in[e - 1], rgt = in[e + 2];
+            T yn[2];
+            if (s == 1)
+                yn[0] = n0[j][0], yn[1] = n0[j][1];
+            else
+                ld_rpair(sYn + pi, yn[0], yn[1]);
+            cx<T> kw[2];
+            T kr[2] = {(T)0, (T)0};
+            rhs_fused<T, RES>(P, s - 1, c0, u0, d0, lft, c1, yn[0], pu[j][0], po[j][0], has_pump, has_pot, kw[0], kr[0]);
+            rhs_fused<T, RES>(P, s - 1, c1, u1, d1, c0, rgt, yn[1], pu[j][1], po[j][1], has_pump, has_pot, kw[1], kr[1]);
+            // k_s of both points (k6: psi only, read by the error stage)
+            sts_pair(sK + ks + pi, kw[0], kw[1]);
+            if constexpr (RES) {
+                if (s <= 5) st_rpair(sKn + ks + pi, kr[0], kr[1]);
+            }
+            // Y_{s+1} = y0 + dt sum_{q<s} w_q k_{q+1}: left to right, zeros included
+            // (runge_sum_to_input_k2..k7); stage 1 the single-weight form
+            cx<T> ynew[2];
+            T nnew[2] = {(T)0, (T)0};
+            if (s == 1) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    ynew[h] = cadd(y0[j][h], smul(P.dtw1, kw[h]));
+                    if constexpr (RES) nnew[h] = radd(n0[j][h], rmul(P.dtw1, kr[h]));
+                }
+            } else {
+                cx<T> a[2];
+                T an[2] = {(T)0, (T)0};
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    if (q >= s) break;
+                    cx<T> k0, k1;
+                    T kn0 = (T)0, kn1 = (T)0;
+                    if (q == s - 1) {
+                        k0 = kw[0], k1 = kw[1];
+                        kn0 = kr[0], kn1 = kr[1];
+                    } else {
+                        const int ki = Lay::kbase(q + 1) - q * W6 + pi;  // k_{q+1}, margin q
+                        lds_pair(sK + ki, k0, k1);
+                        if constexpr (RES) ld_rpair(sKn + ki, kn0, kn1);
+                    }
+                    const T wq = P.w[s - 1][q];
+                    if (q == 0) {
+                        a[0] = smul(wq, k0), a[1] = smul(wq, k1);
+                        an[0] = rmul(wq, kn0), an[1] = rmul(wq, kn1);
+                    } else {
+                        a[0] = cadd(a[0], smul(wq, k0)), a[1] = cadd(a[1], smul(wq, k1));
+                        an[0] = radd(an[0], rmul(wq, kn0)), an[1] = radd(an[1], rmul(wq, kn1));
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    ynew[h] = cadd(y0[j][h], smul(P.dt, a[h]));
+                    if constexpr (RES) nnew[h] = radd(n0[j][h], rmul(P.dt, an[h]));
+                }
+            }
+            sts_pair(out + e, ynew[0], ynew[1]);
+            if constexpr (RES) st_rpair(sYn + pi, nnew[0], nnew[1]);
+            // reference-norm ring cells whose last stage is this one (rho = 7 - s)
+            if (ring_tile) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int x = qx + h;
+                    if (x < m || x >= W6 - m) continue;
+                    const int gy = ty0 - 6 + qy, gx = tx0 - 6 + x;
+                    const int dr = gy < 0 ? -gy : (gy >= P.N_r ? gy - P.N_r + 1 : 0);
+                    const int dc = gx < 0 ? -gx : (gx >= P.N_c ? gx - P.N_c + 1 : 0);
+                    const int cy = min(max(gy, 0), P.N_r - 1), cxp = min(max(gx, 0), P.N_c - 1);
+                    if (max(dr, dc) != kDpH - s || cy < ty0 || cy >= ty0 + TH || cxp < tx0 || cxp >= tx0 + TW) continue;
+                    cx<T> ee = mk((T)0, (T)0);
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) {
+                        if (q >= s) break;
+                        if (P.e[q] == (T)0) continue;
+                        const cx<T> kq = q == s - 1 ? kw[h] : sK[Lay::kbase(q + 1) - q * W6 + pi + h];
+                        ee = cadd(ee, smul(P.e[q], kq));
+                    }
+                    err_acc += (double)abs2(smul(P.dt, ee));
+                    nrm_acc += (double)abs2(ynew[h]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // 4) stage 7 over the tile: k7 = f(Y7), error and norm of the grid points,
+    // the solution written out with its periodic images
+    {
+        const cx<T>* in = sY0;  // Y7 (written by stage 6)
+#pragma unroll
+        for (int j = 0; j < OWN; ++j) {
+            const int p = threadIdx.x + NT * j;
+            const int qy = p / PW, qx = 2 * (p - qy * PW);
+            if (p >= NP || qy < 6 || qy >= H6 - 6 || qx + 1 < 6 || qx >= W6 - 6) continue;
+            const int e = (qy + 1) * SW + qx + 2;
+            const int pi = qy * W6 + qx;
+            cx<T> c0, c1, u0, u1, d0, d1;
+            lds_pair(in + e, c0, c1);
+            lds_pair(in + e - SW, u0, u1);
+            lds_pair(in + e + SW, d0, d1);
+            const cx<T> lft = in[e - 1], rgt = in[e + 2];
+            T yn[2];
+            ld_rpair(sYn + pi, yn[0], yn[1]);
+            cx<T> kw[2];
+            T kr[2] = {(T)0, (T)0};
+            rhs_fused<T, RES>(P, 6, c0, u0, d0, lft, c1, yn[0], pu[j][0], po[j][0], has_pump, has_pot, kw[0], kr[0]);
+            rhs_fused<T, RES>(P, 6, c1, u1, d1, c0, rgt, yn[1], pu[j][1], po[j][1], has_pump, has_pot, kw[1], kr[1]);
+            cx<T> ee[2] = {mk((T)0, (T)0), mk((T)0, (T)0)};
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                if (P.e[q] == (T)0) continue;
+                cx<T> k0, k1;
+                if (q == 6) {
+                    k0 = kw[0], k1 = kw[1];
+                } else {
+                    lds_pair(sK + Lay::kbase(q + 1) - q * W6 + pi, k0, k1);
+                }
+                ee[0] = cadd(ee[0], smul(P.e[q], k0));
+                ee[1] = cadd(ee[1], smul(P.e[q], k1));
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int x = qx + h;
+                if (x < 6 || x >= W6 - 6) continue;
+                const int gy = ty0 - 6 + qy, gx = tx0 - 6 + x;
+                if (gy >= P.N_r || gx >= P.N_c) continue;
+                const cx<T> yc = h == 0 ? c0 : c1;
+                err_acc += (double)abs2(smul(P.dt, ee[h]));
+                nrm_acc += (double)abs2(yc);
+                const long long g = (long long)gy * pitch + gx;
+                P.psi1[g] = yc;
+                if constexpr (RES) P.n1[g] = yn[h];
+                // periodic images kDpImg deep (the next attempt reads tile + 7)
+                const bool lx = P.img_x && gx < kDpImg, hx = P.img_x && gx >= P.N_c - kDpImg;
+                const bool ly = P.img_y && gy < kDpImg, hy = P.img_y && gy >= P.N_r - kDpImg;
+                if (lx || hx || ly || hy) {
+                    const int cs = lx ? gx + P.N_c : gx - P.N_c;
+                    const int rs = ly ? gy + P.N_r : gy - P.N_r;
+                    if (lx || hx) {
+                        P.psi1[(long long)gy * pitch + cs] = yc;
+                        if constexpr (RES) P.n1[(long long)gy * pitch + cs] = yn[h];
+                    }
+                    if (ly || hy) {
+                        P.psi1[(long long)rs * pitch + gx] = yc;
+                        if constexpr (RES) P.n1[(long long)rs * pitch + gx] = yn[h];
+                    }
+                    if ((lx || hx) && (ly || hy)) {
+                        P.psi1[(long long)rs * pitch + cs] = yc;
+                        if constexpr (RES) P.n1[(long long)rs * pitch + cs] = yn[h];
+                    }
+                }
+            }
+        }
+    }
+    __shared__ double red[2 * (NT / 32)];
+    block_reduce2<NT>(err_acc, nrm_acc, red);
+    if (threadIdx.x == 0) {
+        const long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+        P.partials[2 * b] = err_acc;
+        P.partials[2 * b + 1] = nrm_acc;
+    }
+}
+
+}  // namespace phx

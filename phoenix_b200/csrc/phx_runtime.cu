@@ -39,6 +39,7 @@
 #include "phx_rt.hpp"
 #include "phx_adjoint.cuh"
 #include "phx_ssfm.cuh"
+#include "phx_dp45_fused.cuh"
 
 namespace phx {
 
@@ -135,7 +136,7 @@ struct Engine final : EngineBase {
     static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
     static constexpr int kFusedShapes = 9;       // shapes 8-12: persistent TMA-fed variants
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + kFusedShapes];
-    static constexpr int kRingBlocks = 64;
+    static constexpr int kRingBlocks = 256;  // blocks of the ring-norm kernels (their partial-sum slots follow the stage kernels')
     static constexpr int kNormBlocks = 296;
     // imaginary-time propagation (--imagTime): k-stack sums with the complex
     // step, then Solver::normalizeImaginaryTimePropagation after every iteration
@@ -232,7 +233,7 @@ struct Engine final : EngineBase {
         }
         long long min_rpb = rows_per_block(0);
         for (int sh = 1; sh < kShapes; ++sh) min_rpb = std::min(min_rpb, rows_per_block(sh));
-        const long long max_blocks = grid_x(-(long long)G, N_c + G) * ((N_r + 2LL * G + min_rpb - 1) / min_rpb) + 64;
+        const long long max_blocks = grid_x(-(long long)G, N_c + G) * ((N_r + 2LL * G + min_rpb - 1) / min_rpb) + kRingBlocks;
         if (const char* e = std::getenv("PHX_STAGE_SHAPE")) {
             const int v = std::atoi(e);
             if (v >= 0 && v < kShapes) shape = v;
@@ -682,10 +683,10 @@ struct Engine final : EngineBase {
     // this iteration needs the per-stage kernels (complex temporal
     // coefficients).
     // fused-iteration tile shapes (TW x TH points, NT threads); FP64 uses half-height tiles
-    template <bool RES, int TW, int TH, int NT>
+    template <bool RES, int TW, int TH, int NT, bool FMA>
     void go_fused_shape(const FusedParams<T>& F) {
         dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
-        rk4_fused_kernel<T, RES, TW, TH, NT><<<grid, NT, 0, stream>>>(F);
+        rk4_fused_kernel<T, RES, TW, TH, NT, false, FMA><<<grid, NT, 0, stream>>>(F);
     }
     // ---- TMA-fed persistent variant
     int sm_count = 0;
@@ -746,10 +747,10 @@ struct Engine final : EngineBase {
         Q.wait_polls = wait_polls;
         if (!sm_count) PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
     }
-    template <bool RES, int TW, int TH, int NT, int MINB = 1>
+    template <bool RES, int TW, int TH, int NT, int MINB, bool FMA>
     void go_tma(const FusedParams<T>& F) {
         using Lay = TmaLayout<T, TW, TH>;
-        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT, MINB>;
+        auto kern = rk4_tma_kernel<T, RES, TW, TH, NT, MINB, false, FMA>;
         int& tma_blocks_per_sm = tma_blocks[reinterpret_cast<const void*>(kern)];
         if (!tma_blocks_per_sm) {
             PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
@@ -772,28 +773,29 @@ struct Engine final : EngineBase {
         }
     }
 
-    template <bool RES>
+    // FMA: the fused multiply-add arithmetic (phx_params.fma, FP32 only)
+    template <bool RES, bool FMA = false>
     void go_fused(const FusedParams<T>& F) {
         constexpr bool f32 = sizeof(T) == 4;
         switch (cur_shape() - kFusedShape) {
-            case 4: go_tma<RES, 32, f32 ? 32 : 16, 256>(F); return;
+            case 4: go_tma<RES, 32, f32 ? 32 : 16, 256, 1, FMA>(F); return;
             // 12 warps per CTA, two CTAs per SM: registers capped at 85
-            case 5: go_tma<RES, 32, f32 ? 32 : 16, 384, 2>(F); return;
-            case 6: go_tma<RES, 64, f32 ? 16 : 8, 384, 2>(F); return;
+            case 5: go_tma<RES, 32, f32 ? 32 : 16, 384, 2, FMA>(F); return;
+            case 6: go_tma<RES, 64, f32 ? 16 : 8, 384, 2, FMA>(F); return;
             // taller tiles, one CTA per SM: less halo recomputation per output point
-            case 7: go_tma<RES, 64, f32 ? 32 : 16, 768>(F); return;
-            case 8: go_tma<RES, 64, f32 ? 32 : 16, 512>(F); return;
+            case 7: go_tma<RES, 64, f32 ? 32 : 16, 768, 1, FMA>(F); return;
+            case 8: go_tma<RES, 64, f32 ? 32 : 16, 512, 1, FMA>(F); return;
             default: break;
         }
         switch (cur_shape() - kFusedShape) {
-            case 0: go_fused_shape<RES, 32, f32 ? 32 : 16, 256>(F); break;
-            case 1: go_fused_shape<RES, 64, f32 ? 16 : 8, 256>(F); break;
-            case 2: go_fused_shape<RES, 32, f32 ? 16 : 8, 128>(F); break;
+            case 0: go_fused_shape<RES, 32, f32 ? 32 : 16, 256, FMA>(F); break;
+            case 1: go_fused_shape<RES, 64, f32 ? 16 : 8, 256, FMA>(F); break;
+            case 2: go_fused_shape<RES, 32, f32 ? 16 : 8, 128, FMA>(F); break;
             default:
                 if constexpr (f32)
-                    go_fused_shape<RES, 64, 32, 512>(F);
+                    go_fused_shape<RES, 64, 32, 512, FMA>(F);
                 else
-                    go_fused_shape<RES, 32, 24, 384>(F);  // 48 KiB static shared-memory limit
+                    go_fused_shape<RES, 32, 24, 384, FMA>(F);  // 48 KiB static shared-memory limit
                 break;
         }
     }
@@ -826,10 +828,22 @@ struct Engine final : EngineBase {
         F.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
         cudaEvent_t a = nullptr;
         prof_begin(a);
-        if (P.use_reservoir)
-            go_fused<true>(F);
-        else
-            go_fused<false>(F);
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (P.fma) {
+                if (P.use_reservoir)
+                    go_fused<true, true>(F);
+                else
+                    go_fused<false, true>(F);
+                done = true;
+            }
+        }
+        if (!done) {
+            if (P.use_reservoir)
+                go_fused<true>(F);
+            else
+                go_fused<false>(F);
+        }
         const double pts = (double)N_r * N_c;
         const double st = sizeof(C) + (P.use_reservoir ? sizeof(T) : 0);
         prof_end(PHX_KERNEL_RK4_FUSED, a,
@@ -1265,6 +1279,95 @@ struct Engine final : EngineBase {
         }
     }
 
+    // ---- DP45 attempt in one launch (phx_dp45_fused.cuh): scalar, at most one
+    // pump and one potential group, no pulse, no noise, real time, real
+    // temporal coefficients; PHX_DP45_FUSED=0 selects the stage kernels
+    static bool dp45_fused_on() {
+        const char* e = std::getenv("PHX_DP45_FUSED");
+        return !(e && e[0] == '0');
+    }
+    bool dp45_fused_eligible() const {
+        return P.iterator == PHX_ITER_DP45 && !P.tetm && !(P.stochastic_amplitude > 0.0) && !imag_time() &&
+               P.n_pump_groups <= 1 && P.n_potential_groups <= 1 && P.n_pulse_groups == 0 && dp45_fused_on();
+    }
+    // the fused kernel reads the state over tile + 7: periodic images must be
+    // 7 deep, which the stage kernels (4 deep) do not leave behind
+    bool state_images_deep = false;
+    bool dp45_fused_set = false;
+    static constexpr int kDpTW = 32, kDpTH = 16, kDpNT = 256;
+    // one attempt; returns the number of (error, norm) partial pairs, or -1
+    // when this attempt needs the stage kernels (complex temporal coefficients)
+    long long dp45_fused_attempt(bool ref_norm) {
+        Dp45Params<T> Q;
+        std::memset(&Q, 0, sizeof(Q));
+        for (int s = 0; s < 7; ++s) {
+            if (P.n_pump_groups) {
+                const auto c = interp<T>(amp_pump[0], next_pump[0], (T)tab.c[s]);
+                if (c.imag() != (T)0) return -1;
+                Q.pump_c[s] = c.real();
+            }
+            if (P.n_potential_groups) {
+                const auto c = interp<T>(amp_pot[0], next_pot[0], (T)tab.c[s]);
+                if (c.imag() != (T)0) return -1;
+                Q.pot_c[s] = c.real();
+            }
+        }
+        if (!state_images_deep && (P.periodic_x || P.periodic_y)) {
+            ring_fill_kernel<C><<<64, 256, 0, stream>>>(cplane(psi[0]), N_r, N_c, pitch, G, P.periodic_x, P.periodic_y);
+            launches += 1;
+            if (P.use_reservoir) {
+                ring_fill_kernel<T><<<64, 256, 0, stream>>>(rplane(nres[0]), N_r, N_c, pitch, G, P.periodic_x,
+                                                            P.periodic_y);
+                launches += 1;
+            }
+        }
+        const StageParams<T> B = base_params(0);
+        Q.N_r = N_r;
+        Q.N_c = N_c;
+        Q.img_x = P.periodic_x;
+        Q.img_y = P.periodic_y;
+        Q.pitch = pitch;
+        Q.psi0 = cplane(psi[0]);
+        Q.n0 = rplane(nres[0]);
+        Q.psi1 = cplane(sbuf_psi[0][sol_slot()]);
+        Q.n1 = rplane(sbuf_n[0][sol_slot()]);
+        Q.pump = P.n_pump_groups ? rplane(pump[0]) : nullptr;
+        Q.pot = P.n_potential_groups ? rplane(pot[0]) : nullptr;
+        Q.m2 = B.m2, Q.odx2 = B.odx2, Q.ody2 = B.ody2, Q.meff = B.meff, Q.ohb = B.ohb;
+        Q.ohb_gc = B.ohb_gc, Q.half_gamma_c = B.half_gamma_c, Q.ohb_gr = B.ohb_gr, Q.half_R = B.half_R;
+        Q.gamma_r = B.gamma_r, Q.R = B.R;
+        for (int m = 0; m < 6; ++m)
+            for (int q = 0; q < row_n(m) && q < 6; ++q) Q.w[m][q] = row_w(m, q);
+        Q.dtw1 = dt * row_w(0, 0);
+        Q.dt = dt;
+        for (int q = 0; q < 7; ++q) Q.e[q] = (T)tab.e[q];
+        Q.ring = ref_norm ? 1 : 0;
+        const unsigned gx = (unsigned)((N_c + kDpTW - 1) / kDpTW), gy = (unsigned)((N_r + kDpTH - 1) / kDpTH);
+        const long long nb = (long long)gx * gy;
+        if (partials.bytes < sizeof(double) * 2 * (size_t)nb) partials.alloc(sizeof(double) * 2 * (size_t)nb, stream);
+        Q.partials = reinterpret_cast<double*>(partials.p);
+        constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
+        using Lay = Dp45Layout<T, kDpTW, kDpTH>;
+        auto kern = P.use_reservoir ? dp45_fused_kernel<T, true, kDpTW, kDpTH, kDpNT, MINB>
+                                    : dp45_fused_kernel<T, false, kDpTW, kDpTH, kDpNT, MINB>;
+        if (!dp45_fused_set) {
+            PHX_CUDA(cudaFuncSetAttribute(dp45_fused_kernel<T, true, kDpTW, kDpTH, kDpNT, MINB>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
+            PHX_CUDA(cudaFuncSetAttribute(dp45_fused_kernel<T, false, kDpTW, kDpTH, kDpNT, MINB>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
+            dp45_fused_set = true;
+        }
+        cudaEvent_t a = nullptr;
+        prof_begin(a);
+        kern<<<dim3(gx, gy), kDpNT, Lay::total, stream>>>(Q);
+        const double pt = 2.0 * (sizeof(C) + (P.use_reservoir ? sizeof(T) : 0.0)) +
+                          sizeof(T) * (P.n_pump_groups + P.n_potential_groups);
+        prof_end(PHX_KERNEL_DP45_FUSED, a, pt * (double)N_r * N_c);
+        ++launches;
+        PHX_CUDA(cudaGetLastError());
+        return nb;
+    }
+
     void step_adaptive(bool adaptive, int64_t& acc, int64_t& rej) {
         if (tab.inverted) return step_inverted(adaptive, acc, rej);
         if (!adaptive) {
@@ -1282,7 +1385,9 @@ struct Engine final : EngineBase {
         bool accept = false;
         int rejections = 0;
         do {
-            const long long nb = adaptive_stages(true, ref_norm);
+            long long nb = dp45_fused_eligible() ? dp45_fused_attempt(ref_norm) : -1;
+            const bool fused_attempt = nb >= 0;
+            if (!fused_attempt) nb = adaptive_stages(true, ref_norm);
             finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), nb,
                                                           reinterpret_cast<double*>(result.p));
             ++launches;
@@ -1305,6 +1410,7 @@ struct Engine final : EngineBase {
                                         "(NaN or Inf in the state)");
             if (accept) {
                 swap_state_with(sol_slot());
+                state_images_deep = fused_attempt;
                 r7_prev = r7_cur;
                 imag_nrm = nrm;
                 ++acc;
@@ -1458,6 +1564,7 @@ struct Engine final : EngineBase {
 
     // ------------------------------------------------------------ FFT filter
     void fft_filter() {
+        state_images_deep = false;  // the scatter path writes images four deep
         for (int q = 0; q < comps; ++q) {
             if (!have_mask[q] && !keep_spectrum) continue;
             const long long N = (long long)N_r * N_c;
@@ -2250,6 +2357,8 @@ void validate(const phx_params& p) {
                                       "variable branches)");
     }
     if (!std::isfinite(p.stochastic_amplitude)) fail(PHX_ERR_INVALID_ARG, "stochastic_amplitude must be finite");
+    if (p.fma != 0 && p.fma != 1) fail(PHX_ERR_INVALID_ARG, "fma must be 0 or 1");
+    if (p.fma && p.dtype != PHX_F32) fail(PHX_ERR_UNSUPPORTED, "the fused multiply-add arithmetic is provided for FP32");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         (void)cudaGetLastError();

@@ -323,3 +323,4 @@ __global__ void __launch_bounds__(NT) rk4_scalar_general_kernel(const __grid_con
 }
 
 }  // namespace phx
+

@@ -156,7 +156,7 @@ struct TileRef {
 // there); the drain of loads still in flight after a failed wait always uses
 // the full bound, so no bulk copy lands in the shared memory of a CTA that
 // has left.
-template <typename T, bool RES, int TW, int TH, int NT, bool BATCH, bool STORE, typename TileOf>
+template <typename T, bool RES, int TW, int TH, int NT, bool BATCH, bool STORE, bool FMA, typename TileOf>
 __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles, int* err, int wait_polls) {
     using Lay = TmaLayout<T, TW, TH>;
     constexpr int W4 = Lay::W4, WR = Lay::WR;
@@ -290,8 +290,8 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
                 const T po0 = has_pot ? s_po[er] : (T)0, po1 = has_pot ? s_po[er + 1] : (T)0;
                 cx<T> kw[2];
                 T kr[2] = {(T)0, (T)0};
-                rhs_fused<T, RES>(P, s, c0, u0, d0, lft, c1, ns[j][0], pu0, po0, has_pump, has_pot, kw[0], kr[0]);
-                rhs_fused<T, RES>(P, s, c1, u1, d1, c0, rgt, ns[j][1], pu1, po1, has_pump, has_pot, kw[1], kr[1]);
+                rhs_iter<T, RES, FMA>(P, s, c0, u0, d0, lft, c1, ns[j][0], pu0, po0, has_pump, has_pot, kw[0], kr[0]);
+                rhs_iter<T, RES, FMA>(P, s, c1, u1, d1, c0, rgt, ns[j][1], pu1, po1, has_pump, has_pot, kw[1], kr[1]);
                 cx<T> o[2];
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -299,12 +299,12 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
                         acc[j][h] = smul(P.b[0], kw[h]);
                         an[j][h] = rmul(P.b[0], kr[h]);
                     } else if (s < 3) {
-                        acc[j][h] = cadd(acc[j][h], smul(P.b[s], kw[h]));
-                        an[j][h] = radd(an[j][h], rmul(P.b[s], kr[h]));
+                        acc[j][h] = axpy<FMA>(P.b[s], kw[h], acc[j][h]);
+                        an[j][h] = raxpy<FMA>(P.b[s], kr[h], an[j][h]);
                     }
                     if (s < 3) {
-                        o[h] = cadd(y0[j][h], smul(P.dtw[s], kw[h]));
-                        if constexpr (RES) ns[j][h] = radd(n0[j][h], rmul(P.dtw[s], kr[h]));
+                        o[h] = axpy<FMA>(P.dtw[s], kw[h], y0[j][h]);
+                        if constexpr (RES) ns[j][h] = raxpy<FMA>(P.dtw[s], kr[h], n0[j][h]);
                         if constexpr (STORE) {
                             const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
                             if (qy >= 3 && qy < H3 - 3 && qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {
@@ -320,12 +320,12 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
                     } else {
                         const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx + h;
                         if (qx + h >= 3 && qx + h < W3 - 3 && gy < P.N_r && gx < P.N_c) {
-                            const cx<T> ynew = cadd(y0[j][h], smul(P.dt, cadd(acc[j][h], smul(P.b[3], kw[h]))));
+                            const cx<T> ynew = final_update<FMA>(P.dt, P.b[3], acc[j][h], kw[h], y0[j][h]);
                             const long long g = (long long)gy * pitch + gx;
                             P.psi1[g] = ynew;
                             if (P.img_x | P.img_y) fused_images(P, P.psi1, gy, gx, ynew);
                             if constexpr (RES) {
-                                const T nnew = radd(n0[j][h], rmul(P.dt, radd(an[j][h], rmul(P.b[3], kr[h]))));
+                                const T nnew = rfinal_update<FMA>(P.dt, P.b[3], an[j][h], kr[h], n0[j][h]);
                                 P.n1[g] = nnew;
                                 if (P.img_x | P.img_y) fused_images(P, P.n1, gy, gx, nnew);
                             }
@@ -346,7 +346,7 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
 // MINB: CTAs per SM the register allocation must leave room for.  STORE: also
 // write the stage values Y2..Y4 of the tile's points (f.st_psi / f.st_n, with
 // periodic images), which the adjoint's backward sweep reads.
-template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1, bool STORE = false>
+template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1, bool STORE = false, bool FMA = false>
 __global__ void __launch_bounds__(NT, MINB) rk4_tma_kernel(const __grid_constant__ TmaParams<T> Q) {
     auto tile_of = [&](int g) {
         TileRef<T> R;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_tma_kernel(const __grid_constant
         R.tx0 = (g % Q.tiles_x) * TW;
         return R;
     };
-    tma_tile_loop<T, RES, TW, TH, NT, false, STORE>(tile_of, Q.n_tiles, Q.err, Q.wait_polls);
+    tma_tile_loop<T, RES, TW, TH, NT, false, STORE, FMA>(tile_of, Q.n_tiles, Q.err, Q.wait_polls);
 }
 
 // ---------------------------------------------------------------- batches
@@ -385,7 +385,7 @@ struct BatchParams {
     int* err;
 };
 
-template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1>
+template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1, bool FMA = false>
 __global__ void __launch_bounds__(NT, MINB) rk4_batch_kernel(const __grid_constant__ BatchParams<T> B) {
     auto tile_of = [&](int g) {
         const BatchInstance<T>& I = B.inst[__ldg(B.tile_inst + g)];
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_batch_kernel(const __grid_consta
         R.tx0 = (local % I.tiles_x) * TW;
         return R;
     };
-    tma_tile_loop<T, RES, TW, TH, NT, true, false>(tile_of, B.n_tiles, B.err, kWaitPolls);
+    tma_tile_loop<T, RES, TW, TH, NT, true, false, FMA>(tile_of, B.n_tiles, B.err, kWaitPolls);
 }
 
 }  // namespace phx

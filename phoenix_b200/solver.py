@@ -66,6 +66,7 @@ class SystemParameters:
     random_seed: int = 0  # key of the counter-based noise generator
     device: int = 0
     imag_time_amplitude: float = 0.0  # --imagTime A; imaginary-time propagation when != 0
+    fma: bool = False  # FP32 one-kernel RK4 with fused multiply-adds (faster, not bit-identical to the reference)
 
     def magic_timestep(self) -> float:
         dx = self.L_x / (self.N_c - 1)
@@ -102,6 +103,7 @@ class SystemParameters:
         p.n_potential_groups = len(self.potential_temporal)
         p.n_pulse_groups = len(self.pulse_temporal)
         p.device = int(self.device)
+        p.fma = int(bool(self.fma))
         return p
 
 

@@ -47,7 +47,8 @@ def test_fused_tetm_iteration_matches_stage_kernels(require_gpu, monkeypatch, dt
     case, fields = make(70, 46, dtype, px, py, dw)
     monkeypatch.setenv("PHX_TETM_FUSED", "1")
     fused, info = run(case, fields, 12)
-    assert info.iterations == 12
+    # one kernel per iteration, plus the ring refills of zero axes after each
+    assert info.iterations == 12 and info.kernel_launches <= 12 * 5
     monkeypatch.setenv("PHX_TETM_FUSED", "0")
     staged, _ = run(case, fields, 12)
     for k in fused:
