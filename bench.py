@@ -577,7 +577,7 @@ def run_configs(pb, torch, device, ref_gpu=True):
         tune(s)
         us, info = _device_us(torch, s, dev, 1000)
         out["rk4_256_f64"] = {"us_per_iteration": us, "iterations": info.iterations, "launch_shape": info.launch_shape,
-                              "reference_gpu_us": rgpu("f64", n, 0.04, 200 * 0.04 * (1 - 1e-9), 1200 * 0.04 * (1 - 1e-9),
+                              "reference_gpu_us": rgpu("f64", n, 0.04, 200 * 0.04 * (1 - 1e-9), 5200 * 0.04 * (1 - 1e-9),
                                                        scalar_loads(wl, mask=False, potential=False), subgrids=1)}
     # config 2: 1024^2 -- FP64 RK4, DP45 adaptive
     n = 1024
@@ -592,7 +592,7 @@ def run_configs(pb, torch, device, ref_gpu=True):
             us, info = _device_us(torch, s, dev, 460)
             out[f"rk4_1024_{dtype}"] = {
                 "us_per_iteration": us, "launch_shape": info.launch_shape,
-                "reference_gpu_us": rgpu(dtype, n, dt, 100 * dt * (1 - 1e-9), 600 * dt * (1 - 1e-9),
+                "reference_gpu_us": rgpu(dtype, n, dt, 100 * dt * (1 - 1e-9), 2100 * dt * (1 - 1e-9),
                                          scalar_loads(wl, mask=False), subgrids=1)}
     dp = ["-adaptive", "--iterator", "DP45", "--tol", "1e-06", "--rkvdt", "1e-05", "0.05"]
     for dtype in ("f32", "f64"):
@@ -607,7 +607,7 @@ def run_configs(pb, torch, device, ref_gpu=True):
             out[f"dp45_adaptive_1024_{dtype}"] = {
                 "us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
                 "accepted": info.accepted, "rejected": info.rejected, "dt": info.dt,
-                "reference_gpu_us": rgpu(dtype, n, dt, 0.2, 0.8, scalar_loads(wl, mask=False), extra=dp, subgrids=1)}
+                "reference_gpu_us": rgpu(dtype, n, dt, 0.2, 2.2, scalar_loads(wl, mask=False), extra=dp, subgrids=1)}
     # config 3: 4096^2 TE/TM FP32
     out.update(run_tetm(pb, torch, dev, 4096))
     if ref_gpu:
@@ -615,7 +615,7 @@ def run_configs(pb, torch, device, ref_gpu=True):
         tetm = ["-tetm", "--gpm", repr(-0.2 * PHYS["g_c"]), "--deltaLT", "0.05", "--initRandom", "0.01", "4",
                 "--pump", repr(1.5 * P_TH), "add", "10", "10", "0", "0", "both", "1", "none", "gauss+noDivide"]
         for key, dw in (("tetm_4096_f32_deterministic", "0"), ("tetm_4096_f32_noise", "0.001")):
-            out[key]["reference_gpu_us"] = rgpu("f32", 4096, dt3, 20 * dt3 * (1 - 1e-9), 70 * dt3 * (1 - 1e-9),
+            out[key]["reference_gpu_us"] = rgpu("f32", 4096, dt3, 20 * dt3 * (1 - 1e-9), 170 * dt3 * (1 - 1e-9),
                                                 extra=tetm + ["--dw", dw], subgrids=16)
     for k, v in out.items():
         mine = v.get("us_per_iteration", v.get("us_per_accepted_step"))
@@ -719,7 +719,8 @@ def main():
                          "fma (phx_params.fma, FP32)")
     ap.add_argument("--ref-iters", type=int, default=400, help="cap on reference CPU iterations")
     ap.add_argument("--cpu-iters", type=int, default=1500, help="CPU-baseline sample in the phx arm (about 10 s)")
-    ap.add_argument("--ref-gpu-iters", type=int, default=500, help="iterations of the reference GPU build")
+    ap.add_argument("--ref-gpu-iters", type=int, default=2000,
+                    help="iterations of the reference GPU build beyond its first 100")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU and GPU builds")
     ap.add_argument("--sweep-instances", type=int, default=256, help="instances of the batched sweep (0: skip)")
     ap.add_argument("--sweep-steps", type=int, default=200, help="timed iterations of the batched sweep")

@@ -165,7 +165,7 @@ typedef struct {
     int64_t fft_filters;            /* k-space mask applications */
     int64_t kernel_launches;        /* this library's kernels launched */
     int32_t launch_shape;           /* launch shape in use: 0-3 per-stage kernels, 4-7 the fused
-                                       RK4 iteration (tile shapes), 8-12 its persistent TMA-fed
+                                       RK4 iteration (tile shapes), 8-13 its persistent TMA-fed
                                        variants, -1 while the first iterations time them */
     int32_t reserved;
 } phx_step_info;

@@ -26,8 +26,11 @@
 // extended regions cover ring cells evaluates exactly those stages there (from
 // periodic images or from the zero ring, as the reference does), so it adds a
 // ring cell's terms at the stage 7 - rho that last reaches it, counting each
-// ring cell in the tile that holds the cell's nearest grid point.  Ring 7 (the
-// previous accepted state) is summed by ring7_kernel.
+// ring cell in the tile that holds the cell's nearest grid point.  Ring 7 of
+// the state (which the reference's norm sees one accepted step later, when its
+// buffers have swapped) is summed from the stencil buffer the same way.  The
+// block that finishes last adds every block's partial sums in a fixed order
+// (no spin-wait: a ticket counter tells a block it is the last).
 #pragma once
 
 #include "phx_stage.cuh"
@@ -56,8 +59,10 @@ struct Dp45Params {
     T dtw1;     // dt * a_21, the single-weight sum of stage 1
     T dt;
     T e[7];     // error weights
-    int ring;   // add the reference-norm rings 1..6
-    double* partials;  // per block (error, norm)
+    int ring;   // add the reference-norm rings 1..6, and sum ring 7 of the state
+    double* partials;  // per block (error, norm, ring 7)
+    unsigned* ticket;  // blocks finished; the last one sums the partials and resets it to 0
+    double* result;    // (error, norm without ring 7, ring 7 of the state), FP64
 };
 
 template <typename T, int TW, int TH>
@@ -81,6 +86,19 @@ struct Dp45Layout {
     static constexpr int kn_off = kp_off + al(kpts * 2 * (int)sizeof(T));
     static constexpr int total = kn_off + al(knpts * (int)sizeof(T)) + 128;
 };
+
+// block sum of one FP64 value (valid in thread 0); smem holds BLOCK / 32 values
+template <int BLOCK>
+__device__ __forceinline__ void block_reduce1(double& a, double* smem) {
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem[warp] = a;
+    __syncthreads();
+    if (warp == 0) {
+        a = lane < BLOCK / 32 ? smem[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    }
+}
 
 // a pair of real values at an even index of a shared array (8 / 16 bytes)
 template <typename T>
@@ -134,6 +152,38 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
         const int gy = min(ty0 - 7 + ry, rmax), gx = min(tx0 - 7 + rx, cmax);
         sY0[ry * SW + rx + 1] = P.psi0[(long long)gy * pitch + gx];
     }
+    double err_acc = 0.0, nrm_acc = 0.0, r7_acc = 0.0;
+    __syncthreads();
+    // ring 7 of the state: |psi|^2 of the cells at distance 7 from the grid
+    // (zero along zero axes, where the loaded ring holds zeros)
+    // only the rows gy = -7, N_r + 6 and the columns gx = -7, N_c + 6 hold such
+    // cells; a cell on one of those rows is counted there, not in the columns
+    if (ring_tile) {
+        for (int i = threadIdx.x; i < 2 * (W7 + H7); i += NT) {
+            int ry, rx;
+            bool on_row;
+            if (i < 2 * W7) {
+                const int k = i / W7;
+                ry = (k == 0 ? -7 : P.N_r + 6) - (ty0 - 7);
+                rx = i - k * W7;
+                on_row = true;
+            } else {
+                const int k = (i - 2 * W7) / H7;
+                rx = (k == 0 ? -7 : P.N_c + 6) - (tx0 - 7);
+                ry = i - 2 * W7 - k * H7;
+                on_row = false;
+            }
+            if (ry < 0 || ry >= H7 || rx < 0 || rx >= W7) continue;
+            const int gy = ty0 - 7 + ry, gx = tx0 - 7 + rx;
+            const int dr = gy < 0 ? -gy : (gy >= P.N_r ? gy - P.N_r + 1 : 0);
+            const int dc = gx < 0 ? -gx : (gx >= P.N_c ? gx - P.N_c + 1 : 0);
+            if (!on_row && dr == kDpH) continue;
+            const int cy = min(max(gy, 0), P.N_r - 1), cxp = min(max(gx, 0), P.N_c - 1);
+            if (max(dr, dc) != kDpH || cy < ty0 || cy >= ty0 + TH || cxp < tx0 || cxp >= tx0 + TW) continue;
+            if ((dr && !P.img_y) || (dc && !P.img_x)) continue;
+            r7_acc += (double)abs2(sY0[ry * SW + rx + 1]);
+        }
+    }
     // 2) pointwise values of the owned pairs (stage-1 region coordinates)
     cx<T> y0[OWN][2];
     T n0[OWN][2], pu[OWN][2], po[OWN][2];
@@ -152,7 +202,6 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
             po[j][h] = (has_pot && own) ? __ldg(P.pot + g) : (T)0;
         }
     }
-    __syncthreads();
 #pragma unroll
     for (int j = 0; j < OWN; ++j) {
         const int p = threadIdx.x + NT * j;
@@ -163,7 +212,6 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
             y0[j][0] = y0[j][1] = mk((T)0, (T)0);
     }
 
-    double err_acc = 0.0, nrm_acc = 0.0;
     // 3) stages 1..6; stage s covers margin s - 1 of the stage-1 region.  A
     // pair straddling the region's x edge computes both points; the outer one
     // is stored but never read as a value the reference computes.
@@ -342,11 +390,37 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
         }
     }
     __shared__ double red[2 * (NT / 32)];
+    __shared__ double red7[NT / 32];
+    __shared__ bool last;
     block_reduce2<NT>(err_acc, nrm_acc, red);
+    block_reduce1<NT>(r7_acc, red7);
+    const unsigned nb = gridDim.x * gridDim.y;
     if (threadIdx.x == 0) {
-        const long long b = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-        P.partials[2 * b] = err_acc;
-        P.partials[2 * b + 1] = nrm_acc;
+        const unsigned b = blockIdx.y * gridDim.x + blockIdx.x;
+        P.partials[3 * b] = err_acc;
+        P.partials[3 * b + 1] = nrm_acc;
+        P.partials[3 * b + 2] = r7_acc;
+        __threadfence();
+        last = atomicAdd(P.ticket, 1u) == nb - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    // the last block: every partial is visible (fence before each ticket); sum
+    // them in a fixed order, whichever block this is
+    __threadfence();
+    double a = 0.0, b2 = 0.0, c = 0.0;
+    for (unsigned i = threadIdx.x; i < nb; i += NT) {
+        a += __ldcg(P.partials + 3 * i);
+        b2 += __ldcg(P.partials + 3 * i + 1);
+        c += __ldcg(P.partials + 3 * i + 2);
+    }
+    block_reduce2<NT>(a, b2, red);
+    block_reduce1<NT>(c, red7);
+    if (threadIdx.x == 0) {
+        P.result[0] = a;
+        P.result[1] = b2;
+        P.result[2] = c;
+        *P.ticket = 0;
     }
 }
 

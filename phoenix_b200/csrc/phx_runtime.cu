@@ -134,7 +134,7 @@ struct Engine final : EngineBase {
     static constexpr int kTuneIters = 3;   // consecutive iterations of one candidate per sample
     static constexpr double kTuneMargin = 0.03;  // a challenger must beat the incumbent by this fraction
     static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
-    static constexpr int kFusedShapes = 9;       // shapes 8-12: persistent TMA-fed variants
+    static constexpr int kFusedShapes = 10;      // shapes 8-13: persistent TMA-fed variants
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + kFusedShapes];
     static constexpr int kRingBlocks = 256;  // blocks of the ring-norm kernels (their partial-sum slots follow the stage kernels')
     static constexpr int kNormBlocks = 296;
@@ -257,7 +257,7 @@ struct Engine final : EngineBase {
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
     // autotuning candidates: the stage kernels' shapes 0-3, or, where the
-    // one-kernel iteration applies, its shapes 4-12 (the stage kernels, four
+    // one-kernel iteration applies, its shapes 4-13 (the stage kernels, four
     // launches and 236 B per point, never beat it there)
     int first_candidate() const { return fused_eligible_static() ? kFusedShape : 0; }
     int n_candidates() const { return fused_eligible_static() ? kFusedShapes : kShapes; }
@@ -785,6 +785,9 @@ struct Engine final : EngineBase {
             // taller tiles, one CTA per SM: less halo recomputation per output point
             case 7: go_tma<RES, 64, f32 ? 32 : 16, 768, 1, FMA>(F); return;
             case 8: go_tma<RES, 64, f32 ? 32 : 16, 512, 1, FMA>(F); return;
+            // 64 x 14: 1024^2 makes 1184 tiles, exactly four rounds of 296 CTAs
+            // (64 x 16 leaves the fourth round half empty)
+            case 9: go_tma<RES, 64, f32 ? 14 : 7, 384, 2, FMA>(F); return;
             default: break;
         }
         switch (cur_shape() - kFusedShape) {
@@ -1294,21 +1297,23 @@ struct Engine final : EngineBase {
     // 7 deep, which the stage kernels (4 deep) do not leave behind
     bool state_images_deep = false;
     bool dp45_fused_set = false;
+    DevBuf dp45_ticket;  // blocks of a fused attempt that have finished (the last one resets it)
     static constexpr int kDpTW = 32, kDpTH = 16, kDpNT = 256;
-    // one attempt; returns the number of (error, norm) partial pairs, or -1
-    // when this attempt needs the stage kernels (complex temporal coefficients)
-    long long dp45_fused_attempt(bool ref_norm) {
+    // one attempt, which leaves (error, norm, ring 7) in `result`; returns
+    // false when this attempt needs the stage kernels (complex temporal
+    // coefficients)
+    bool dp45_fused_attempt(bool ref_norm) {
         Dp45Params<T> Q;
         std::memset(&Q, 0, sizeof(Q));
         for (int s = 0; s < 7; ++s) {
             if (P.n_pump_groups) {
                 const auto c = interp<T>(amp_pump[0], next_pump[0], (T)tab.c[s]);
-                if (c.imag() != (T)0) return -1;
+                if (c.imag() != (T)0) return false;
                 Q.pump_c[s] = c.real();
             }
             if (P.n_potential_groups) {
                 const auto c = interp<T>(amp_pot[0], next_pot[0], (T)tab.c[s]);
-                if (c.imag() != (T)0) return -1;
+                if (c.imag() != (T)0) return false;
                 Q.pot_c[s] = c.real();
             }
         }
@@ -1344,8 +1349,11 @@ struct Engine final : EngineBase {
         Q.ring = ref_norm ? 1 : 0;
         const unsigned gx = (unsigned)((N_c + kDpTW - 1) / kDpTW), gy = (unsigned)((N_r + kDpTH - 1) / kDpTH);
         const long long nb = (long long)gx * gy;
-        if (partials.bytes < sizeof(double) * 2 * (size_t)nb) partials.alloc(sizeof(double) * 2 * (size_t)nb, stream);
+        if (partials.bytes < sizeof(double) * 3 * (size_t)nb) partials.alloc(sizeof(double) * 3 * (size_t)nb, stream);
+        if (!dp45_ticket.p) dp45_ticket.alloc(sizeof(unsigned), stream);  // zeroed; the kernel leaves it at 0
         Q.partials = reinterpret_cast<double*>(partials.p);
+        Q.ticket = static_cast<unsigned*>(dp45_ticket.p);
+        Q.result = reinterpret_cast<double*>(result.p);
         constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
         using Lay = Dp45Layout<T, kDpTW, kDpTH>;
         auto kern = P.use_reservoir ? dp45_fused_kernel<T, true, kDpTW, kDpTH, kDpNT, MINB>
@@ -1365,7 +1373,7 @@ struct Engine final : EngineBase {
         prof_end(PHX_KERNEL_DP45_FUSED, a, pt * (double)N_r * N_c);
         ++launches;
         PHX_CUDA(cudaGetLastError());
-        return nb;
+        return true;
     }
 
     void step_adaptive(bool adaptive, int64_t& acc, int64_t& rej) {
@@ -1375,23 +1383,25 @@ struct Engine final : EngineBase {
             return;
         }
         const bool ref_norm = P.norm_mode == PHX_NORM_REFERENCE;
-        if (ref_norm) {
-            // outer ring H of the state's halo at the start of this step -> result[2]
-            ring7_kernel<T><<<1, 1024, 0, stream>>>(cplane(psi[0]), pitch, N_r, N_c, P.periodic_x, P.periodic_y, H,
-                                                    reinterpret_cast<double*>(result.p) + 2);
-            ++launches;
-            PHX_CUDA(cudaGetLastError());
-        }
-        bool accept = false;
+        bool accept = false, ring7_done = false;
         int rejections = 0;
         do {
-            long long nb = dp45_fused_eligible() ? dp45_fused_attempt(ref_norm) : -1;
-            const bool fused_attempt = nb >= 0;
-            if (!fused_attempt) nb = adaptive_stages(true, ref_norm);
-            finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), nb,
-                                                          reinterpret_cast<double*>(result.p));
-            ++launches;
-            PHX_CUDA(cudaGetLastError());
+            // the fused attempt sums its norms (ring 7 included) in the same launch
+            const bool fused_attempt = dp45_fused_eligible() && dp45_fused_attempt(ref_norm);
+            if (!fused_attempt) {
+                if (ref_norm && !ring7_done) {
+                    // outer ring H of the state's halo at the start of this step -> result[2]
+                    ring7_kernel<T><<<1, 1024, 0, stream>>>(cplane(psi[0]), pitch, N_r, N_c, P.periodic_x,
+                                                            P.periodic_y, H, reinterpret_cast<double*>(result.p) + 2);
+                    ++launches;
+                    ring7_done = true;
+                }
+                const long long nb = adaptive_stages(true, ref_norm);
+                finalize_pairs_kernel<<<1, 1024, 0, stream>>>(reinterpret_cast<double*>(partials.p), nb,
+                                                              reinterpret_cast<double*>(result.p));
+                ++launches;
+                PHX_CUDA(cudaGetLastError());
+            }
             PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
             PHX_CUDA(cudaStreamSynchronize(stream));
             const double* r = static_cast<const double*>(host_result.p);

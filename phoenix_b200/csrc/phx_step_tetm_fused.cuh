@@ -119,9 +119,15 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
         cx<T>* op = pbuf(ob, 0);
         cx<T>* om = pbuf(ob, 1);
         const int ws = W3 - 2 * s, n_items = ws * (H3 - 2 * s);
+        // the item's (row, column) in the stage's region, advanced by NT items
+        // per pass without a division per item
+        const int adv_r = NT / ws, adv_c = NT - adv_r * ws;
+        int ir = threadIdx.x / ws, ic = threadIdx.x - ir * ws;
 #pragma unroll 1
         for (int it = threadIdx.x; it < n_items; it += NT) {
-            const int qy = s + it / ws, qx = s + it % ws;
+            const int qy = s + ir, qx = s + ic;
+            ir += adv_r, ic += adv_c;
+            if (ic >= ws) ic -= ws, ++ir;
             const int q = qy * W3 + qx;                // tile + 3 index
             const int e = (qy + 1) * SW + qx + 2;      // shared psi index
             const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx;
@@ -265,9 +271,13 @@ __global__ void __launch_bounds__(NT) rk4_scalar_general_kernel(const __grid_con
         const cx<T>* in = pbuf(ib);
         cx<T>* out = pbuf(ob);
         const int ws = W3 - 2 * s, n_items = ws * (H3 - 2 * s);
+        const int adv_r = NT / ws, adv_c = NT - adv_r * ws;
+        int ir = threadIdx.x / ws, ic = threadIdx.x - ir * ws;
 #pragma unroll 1
         for (int it = threadIdx.x; it < n_items; it += NT) {
-            const int qy = s + it / ws, qx = s + it % ws;
+            const int qy = s + ir, qx = s + ic;
+            ir += adv_r, ic += adv_c;
+            if (ic >= ws) ic -= ws, ++ir;
             const int q = qy * W3 + qx;
             const int e = (qy + 1) * SW + qx + 2;
             const int gy = ty0 - 3 + qy, gx = tx0 - 3 + qx;
