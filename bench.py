@@ -11,15 +11,19 @@ amplitude 1e-2, n0 = 0.
 
 Legs of the JSON line:
   value      device time per iteration (CUDA events on the solver's stream),
-             L2 flushed (256 MiB write) between timed iterations, max over ranks
+             L2 flushed (256 MiB write, then read) between timed iterations, max
+             over ranks; the library's own per-launch events are off in this pass
   e2e        the same workload through the public API with host buffers:
              upload psi0/n0 from pinned host memory, run in chunks of 100
              iterations reading the FP64 norm back after each chunk, download
              psi and n into pinned host memory at the end (after one untimed
              pass of the same sequence on the same handle and buffers)
-  roofline   the dominant kernel (fused RK4 stage 2/3) from per-launch CUDA
-             events recorded by the library on its stream during the timed
-             region: algorithmic bytes / average duration vs measured HBM peak
+  roofline   the dominant kernel (the one-kernel RK4 iteration) from per-launch
+             CUDA events the library records on its stream during a second,
+             identical timed pass: algorithmic bytes / average duration vs the
+             measured HBM peak
+  fma        the same workload and timing with phx_params.fma = 1 (FP32)
+  autotune   the launch shape the library's tuner kept and its per-shape medians
   cpu_baseline  the reference's CPU build (PHOENIX compiled from its sources,
              oracle/_ref) on a bounded sample of the same workload, all host cores
   sweep      the batched sweep: 256 independent 128^2..1024^2 FP32 instances
@@ -29,7 +33,9 @@ Legs of the JSON line:
   adjoint    the inverse-design gradient: 512^2 FP32, 500 RK4 iterations, device
              time of the plain forward, the checkpointed forward and the backward
   configs    the other configurations: 256^2 FP64 RK4, 1024^2 FP64 RK4 and DP45
-             adaptive (FP32, FP64), FP32-vs-FP64 error, 4096^2 TE/TM FP32 with noise
+             adaptive (FP32, FP64), 4096^2 TE/TM FP32 with noise and without, each
+             beside the reference's own CUDA build (marginal time per iteration),
+             and the FP32-vs-FP64 error of every configuration at its own size
 `--impl reference` runs that reference CPU build alone (rank 0 of any launch).
 """
 from __future__ import annotations
@@ -533,8 +539,9 @@ def run_dp45(pb, torch, dev, n, dtype, steps):
         s.set_field("pump_plus", wl["pump"], 0)
         s.set_field("potential_plus", wl["potential"], 0)
         tune(s)
+        us, info = _device_us(torch, s, dev, steps)  # without the library's own events
         s.profile(True)
-        us, info = _device_us(torch, s, dev, steps)
+        _device_us(torch, s, dev, steps)
         kernels = {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"]}
                    for k, v in s.profile_read().items()}
     return {"grid": n, "dtype": dtype, "us_per_accepted_step": us * info.iterations / max(info.accepted, 1),
@@ -800,26 +807,39 @@ def main():
     smi_index = idx[local] if len(idx) > local and idx[local].strip().isdigit() else str(local)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    launches = 0
-    filters = 0
-    shape = -1
-    solver.profile(True)
-    with ClockSampler(smi_index) as clocks, torch.cuda.stream(stream):
-        # an untimed ~25 ms device sleep lets the host queue the timed
-        # iterations ahead of the GPU, so that no event pair spans host time
-        torch.cuda._sleep(50_000_000)
-        for i in range(args.steps):
-            flush_l2(flush)
-            starts[i].record(stream)
-            info = solver.run(1)
-            ends[i].record(stream)
-            shape = info.launch_shape
-            launches += info.kernel_launches
-            filters += info.fft_filters
-        torch.cuda.synchronize()
-    prof = solver.profile_read()
-    solver.profile(False)
-    step_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
+
+    def timed_pass(profile):
+        """args.steps iterations, L2 flushed before each, each bracketed by an
+        event pair; with profile the library also brackets each of its own
+        launches (the per-kernel times of the roofline)"""
+        launches = filters = 0
+        shape = -1
+        if profile:
+            solver.profile(True)
+        with torch.cuda.stream(stream):
+            # an untimed ~25 ms device sleep lets the host queue the timed
+            # iterations ahead of the GPU, so that no event pair spans host time
+            torch.cuda._sleep(50_000_000)
+            for i in range(args.steps):
+                flush_l2(flush)
+                starts[i].record(stream)
+                info = solver.run(1)
+                ends[i].record(stream)
+                shape = info.launch_shape
+                launches += info.kernel_launches
+                filters += info.fft_filters
+            torch.cuda.synchronize()
+        prof = None
+        if profile:
+            prof = solver.profile_read()
+            solver.profile(False)
+        return sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps, prof, launches, filters, shape
+
+    # the timed region of `value` runs without the library's own events; a
+    # second pass of the same loop with them gives the per-kernel times
+    with ClockSampler(smi_index) as clocks:
+        step_ms, _, launches, filters, shape = timed_pass(False)
+    prof_step_ms, prof, _, _, _ = timed_pass(True)
     t_local = torch.tensor([step_ms], dtype=torch.float64, device=f"cuda:{local}")
     if dist:
         dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
@@ -857,18 +877,28 @@ def main():
         torch.cuda.synchronize()
         fs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         fe = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        sf.profile(True)
-        with torch.cuda.stream(fstream):
-            torch.cuda._sleep(50_000_000)
-            for i in range(args.steps):
-                flush_l2(flush)
-                fs[i].record(fstream)
-                finfo = sf.run(1)
-                fe[i].record(fstream)
-            torch.cuda.synchronize()
-        fprof = sf.profile_read()
+
+        def fma_pass(profile):
+            if profile:
+                sf.profile(True)
+            with torch.cuda.stream(fstream):
+                torch.cuda._sleep(50_000_000)
+                for i in range(args.steps):
+                    flush_l2(flush)
+                    fs[i].record(fstream)
+                    info_ = sf.run(1)
+                    fe[i].record(fstream)
+                torch.cuda.synchronize()
+            pr = None
+            if profile:
+                pr = sf.profile_read()
+                sf.profile(False)
+            return sum(a.elapsed_time(b) for a, b in zip(fs, fe)) / args.steps, pr, info_
+
+        # timed without the library's own events, as the headline; then profiled
+        f_ms, _, finfo = fma_pass(False)
+        _, fprof, _ = fma_pass(True)
         sf.close()
-        f_ms = sum(a.elapsed_time(b) for a, b in zip(fs, fe)) / args.steps
         fk = fprof.get("rk4_fused")
         fma_leg = {"value": f_ms * 1e3, "unit": "us/iter", "launch_shape": finfo.launch_shape,
                    "kernel_avg_ms": fk["ms"] / fk["launches"] if fk else None,
@@ -1001,6 +1031,7 @@ def main():
                 "vs_baseline": None, "dtype": args.dtype, "data": "synthetic", "config": config_dict(args),
                 "grid_point_updates_per_s": world * n * n / (step_ms * 1e-3),
                 "warm_l2_us_per_iter": warm_ms * 1e3,
+                "us_per_iter_with_library_events": prof_step_ms * 1e3,
                 "e2e": {"value": e2e_ms * 1e3, "unit": "us/iter", "h2d_bytes_per_step": h2d / e2e_iters,
                         "d2h_bytes_per_step": d2h / e2e_iters},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
