@@ -184,12 +184,16 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
             r7_acc += (double)abs2(sY0[ry * SW + rx + 1]);
         }
     }
-    // 2) pointwise values of the owned pairs (stage-1 region coordinates)
+    // 2) pointwise values of the owned pairs (stage-1 region coordinates): slot
+    // j of a thread holds pair threadIdx.x + NT * j in row-major order
+    int pidx[OWN];
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) pidx[j] = min((int)threadIdx.x + NT * j, NP);
     cx<T> y0[OWN][2];
     T n0[OWN][2], pu[OWN][2], po[OWN][2];
 #pragma unroll
     for (int j = 0; j < OWN; ++j) {
-        const int p = threadIdx.x + NT * j;
+        const int p = pidx[j];
         const int qy = p / PW, qx = 2 * (p - qy * PW);
         const bool own = p < NP;
         const int gy = min(ty0 - 6 + qy, rmax);
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
     }
 #pragma unroll
     for (int j = 0; j < OWN; ++j) {
-        const int p = threadIdx.x + NT * j;
+        const int p = pidx[j];
         const int qy = p / PW, qx = 2 * (p - qy * PW);
         if (p < NP)
             lds_pair(sY0 + (qy + 1) * SW + qx + 2, y0[j][0], y0[j][1]);
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
         const int ks = Lay::kbase(s) - m * W6;  // k_s row qy at ks + qy * W6
 #pragma unroll
         for (int j = 0; j < OWN; ++j) {
-            const int p = threadIdx.x + NT * j;
+            const int p = pidx[j];
             const int qy = p / PW, qx = 2 * (p - qy * PW);
             if (p >= NP || qy < m || qy >= H6 - m || qx + 1 < m || qx >= W6 - m) continue;
             const int e = (qy + 1) * SW + qx + 2;  // stencil buffer index of the pair (even)
@@ -326,7 +330,7 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
         const cx<T>* in = sY0;  // Y7 (written by stage 6)
 #pragma unroll
         for (int j = 0; j < OWN; ++j) {
-            const int p = threadIdx.x + NT * j;
+            const int p = pidx[j];
             const int qy = p / PW, qx = 2 * (p - qy * PW);
             if (p >= NP || qy < 6 || qy >= H6 - 6 || qx + 1 < 6 || qx >= W6 - 6) continue;
             const int e = (qy + 1) * SW + qx + 2;

@@ -1298,7 +1298,11 @@ struct Engine final : EngineBase {
     bool state_images_deep = false;
     bool dp45_fused_set = false;
     DevBuf dp45_ticket;  // blocks of a fused attempt that have finished (the last one resets it)
-    static constexpr int kDpTW = 32, kDpTH = 16, kDpNT = 256;
+    static constexpr int kDpTW = 32, kDpTH = 16;
+    // FP32: 10 warps, two CTAs per SM (two pair slots per thread: the per-stage
+    // pair counts spread over fewer idle slots than with 8 warps and three);
+    // FP64: 8 warps, one CTA per SM
+    static constexpr int kDpNT = sizeof(T) == 4 ? 320 : 256;
     // one attempt, which leaves (error, norm, ring 7) in `result`; returns
     // false when this attempt needs the stage kernels (complex temporal
     // coefficients)
