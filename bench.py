@@ -472,6 +472,14 @@ def flush_l2(buf):
     buf.view(-1, 4096).amax(dim=1)
 
 
+def max_over_ranks(torch, dist, value, device):
+    """The largest of every rank's value (all ranks call it; dist None: one process)."""
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def tune(solver, cap=600):
     """Run single iterations until the library's launch-shape autotuning has
     ended (launch_shape >= 0); returns the iterations run."""
@@ -840,10 +848,7 @@ def main():
     with ClockSampler(smi_index) as clocks:
         step_ms, _, launches, filters, shape = timed_pass(False)
     prof_step_ms, prof, _, _, _ = timed_pass(True)
-    t_local = torch.tensor([step_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
-    step_ms = float(t_local.item())
+    step_ms = max_over_ranks(torch, dist, step_ms, f"cuda:{local}")
 
     # back-to-back (L2-warm) iterations, one event pair
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1014,14 +1019,16 @@ def main():
                                "clock of its main loop per iteration between the two runs (its Total Runtime / "
                                "mus/it lines)"}
 
+    # the single-GPU legs run at N = 1 only (with N > 1 the other ranks would
+    # wait for them at the closing barrier)
     sweep = None
-    if rank == 0 and args.sweep_instances > 0:
+    if rank == 0 and world == 1 and args.sweep_instances > 0:
         sweep = run_sweep(pb, torch, args.sweep_instances, args.sweep_steps, local)
     adjoint = None
-    if rank == 0 and not args.no_adjoint:
+    if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = run_adjoint(pb, torch, local)
     configs = None
-    if rank == 0 and not args.no_configs:
+    if rank == 0 and world == 1 and not args.no_configs:
         configs = run_configs(pb, torch, local)
 
     if rank == 0:
