@@ -1384,6 +1384,7 @@ struct Engine final : EngineBase {
         if (tab.inverted) return step_inverted(adaptive, acc, rej);
         if (!adaptive) {
             adaptive_stages(false);
+            state_images_deep = false;  // the final stage kernel writes images four deep
             return;
         }
         const bool ref_norm = P.norm_mode == PHX_NORM_REFERENCE;

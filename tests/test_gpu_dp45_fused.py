@@ -9,10 +9,13 @@ later step sizes agree to rounding.  Grids that are not multiples of the
 extended stage regions and the reference-norm rings that edge tiles add),
 FP32 and FP64, both norm modes.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
 import phoenix_b200 as pb
+from phoenix_b200 import _lib as L
 from oracle import phx_oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -97,3 +100,25 @@ def test_complex_potential_envelope_falls_back_to_stage_kernels(require_gpu, mon
     b = run(c, f, monkeypatch, False)
     assert "dp45_fused" not in a[3]
     np.testing.assert_array_equal(a[0], b[0])
+
+
+@pytest.mark.parametrize("bc", [(1, 1), (0, 0)], ids=["periodic", "zero"])
+def test_forced_fixed_steps_between_fused_attempts(require_gpu, monkeypatch, bc):
+    """phx_iterate(force_fixed_time_step) runs a fixed DP45 step on the stage
+    kernels (the main loop's step onto an output time), which write the state's
+    periodic images four deep; the next one-kernel attempt reads seven.  Mixed
+    sequences give the same bits as the stage kernels alone."""
+    c = case(66, 40, bc[0], bc[1], "f64", 1e9, 35)
+    f = fields(c)
+    outs = []
+    for fused in (True, False):
+        monkeypatch.setenv("PHX_DP45_FUSED", "1" if fused else "0")
+        sp = pb.system_from_case(c)
+        with pb.SolverFactory.create(sp) as s:
+            pb.load_case_fields(s, c, f)
+            for k in range(9):
+                info = L.StepInfo()
+                L.check(s._lib.phx_iterate(s._h, 1 if k % 3 == 2 else 0, C.byref(info)), s._h)
+            outs.append((s.get_field("psi_plus"), s.get_field("n_plus"), s.t, s.dt))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
