@@ -107,7 +107,9 @@ def test_forced_fixed_steps_between_fused_attempts(require_gpu, monkeypatch, bc)
     """phx_iterate(force_fixed_time_step) runs a fixed DP45 step on the stage
     kernels (the main loop's step onto an output time), which write the state's
     periodic images four deep; the next one-kernel attempt reads seven.  Mixed
-    sequences give the same bits as the stage kernels alone."""
+    sequences agree with the stage kernels alone to the rounding of the FP64
+    norm sums (which set later step sizes); images left stale three rings deep
+    would differ by about dt times the right-hand side."""
     c = case(66, 40, bc[0], bc[1], "f64", 1e9, 35)
     f = fields(c)
     outs = []
@@ -120,5 +122,7 @@ def test_forced_fixed_steps_between_fused_attempts(require_gpu, monkeypatch, bc)
                 info = L.StepInfo()
                 L.check(s._lib.phx_iterate(s._h, 1 if k % 3 == 2 else 0, C.byref(info)), s._h)
             outs.append((s.get_field("psi_plus"), s.get_field("n_plus"), s.t, s.dt))
-    np.testing.assert_array_equal(outs[0][0], outs[1][0])
-    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    for a, b in ((outs[0][0], outs[1][0]), (outs[0][1], outs[1][1])):
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * np.abs(b).max())
+    assert outs[0][2] == pytest.approx(outs[1][2], rel=1e-12)
+    assert outs[0][3] == pytest.approx(outs[1][3], rel=1e-10)
