@@ -146,11 +146,50 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
     // only tiles at the grid's border hold reference-norm ring cells
     const bool ring_tile = P.ring && (tx0 == 0 || ty0 == 0 || tx0 + TW >= P.N_c || ty0 + TH >= P.N_r);
 
-    // 1) psi0 over tile + 7 into sY0: point (ry, rx) at ry * SW + rx + 1
-    for (int i = threadIdx.x; i < H7 * W7; i += NT) {
-        const int ry = i / W7, rx = i - ry * W7;
-        const int gy = min(ty0 - 7 + ry, rmax), gx = min(tx0 - 7 + rx, cmax);
-        sY0[ry * SW + rx + 1] = P.psi0[(long long)gy * pitch + gx];
+    // 1) psi0 over tile + 7 into sY0 (point (ry, rx) at ry * SW + rx + 1) and
+    // the pointwise inputs of the owned pairs into registers.  A thread issues
+    // all these loads before its first shared store, so that their latencies
+    // overlap (a load-store loop waits for each in turn).
+    constexpr int NL0 = (H7 * W7 + NT - 1) / NT;
+    cx<T> v0[NL0];
+#pragma unroll
+    for (int k = 0; k < NL0; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H7 * W7) {
+            const int ry = i / W7, rx = i - ry * W7;
+            const int gy = min(ty0 - 7 + ry, rmax), gx = min(tx0 - 7 + rx, cmax);
+            v0[k] = P.psi0[(long long)gy * pitch + gx];
+        }
+    }
+    // pointwise values of the owned pairs (stage-1 region coordinates): slot
+    // j of a thread holds pair threadIdx.x + NT * j in row-major order
+    int pidx[OWN];
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) pidx[j] = min((int)threadIdx.x + NT * j, NP);
+    cx<T> y0[OWN][2];
+    T n0[OWN][2], pu[OWN][2], po[OWN][2];
+#pragma unroll
+    for (int j = 0; j < OWN; ++j) {
+        const int p = pidx[j];
+        const int qy = p / PW, qx = 2 * (p - qy * PW);
+        const bool own = p < NP;
+        const int gy = min(ty0 - 6 + qy, rmax);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int gx = min(tx0 - 6 + qx + h, cmax);
+            const long long g = (long long)gy * pitch + gx;
+            n0[j][h] = (RES && own) ? __ldg(P.n0 + g) : (T)0;
+            pu[j][h] = (RES && has_pump && own) ? __ldg(P.pump + g) : (T)0;
+            po[j][h] = (has_pot && own) ? __ldg(P.pot + g) : (T)0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NL0; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H7 * W7) {
+            const int ry = i / W7, rx = i - ry * W7;
+            sY0[ry * SW + rx + 1] = v0[k];
+        }
     }
     double err_acc = 0.0, nrm_acc = 0.0, r7_acc = 0.0;
     __syncthreads();
@@ -182,28 +221,6 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
             if (max(dr, dc) != kDpH || cy < ty0 || cy >= ty0 + TH || cxp < tx0 || cxp >= tx0 + TW) continue;
             if ((dr && !P.img_y) || (dc && !P.img_x)) continue;
             r7_acc += (double)abs2(sY0[ry * SW + rx + 1]);
-        }
-    }
-    // 2) pointwise values of the owned pairs (stage-1 region coordinates): slot
-    // j of a thread holds pair threadIdx.x + NT * j in row-major order
-    int pidx[OWN];
-#pragma unroll
-    for (int j = 0; j < OWN; ++j) pidx[j] = min((int)threadIdx.x + NT * j, NP);
-    cx<T> y0[OWN][2];
-    T n0[OWN][2], pu[OWN][2], po[OWN][2];
-#pragma unroll
-    for (int j = 0; j < OWN; ++j) {
-        const int p = pidx[j];
-        const int qy = p / PW, qx = 2 * (p - qy * PW);
-        const bool own = p < NP;
-        const int gy = min(ty0 - 6 + qy, rmax);
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int gx = min(tx0 - 6 + qx + h, cmax);
-            const long long g = (long long)gy * pitch + gx;
-            n0[j][h] = (RES && own) ? __ldg(P.n0 + g) : (T)0;
-            pu[j][h] = (RES && has_pump && own) ? __ldg(P.pump + g) : (T)0;
-            po[j][h] = (has_pot && own) ? __ldg(P.pot + g) : (T)0;
         }
     }
 #pragma unroll

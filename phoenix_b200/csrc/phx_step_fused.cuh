@@ -185,11 +185,18 @@ __global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ F
     const bool has_pump = P.pump != nullptr, has_pot = P.pot != nullptr;
     const int rmax = P.N_r + kRing - 1, cmax = P.N_c + kRing - 1;
 
-    // 1) psi0 over tile + 4 into sA; R4 point (ry, rx) at sA[ry * SW + rx + 1]
-    for (int i = threadIdx.x; i < H4 * W4; i += NT) {
-        const int ry = i / W4, rx = i - ry * W4;
-        const int gy = min(ty0 - 4 + ry, rmax), gx = min(tx0 - 4 + rx, cmax);
-        sA[ry * SW + rx + 1] = P.psi0[(long long)gy * pitch + gx];
+    // 1) psi0 over tile + 4 into sA; R4 point (ry, rx) at sA[ry * SW + rx + 1].
+    // The loads (and those of the pointwise values below) are all issued
+    // before the first shared store, so that their latencies overlap.
+    constexpr int NL = (H4 * W4 + NT - 1) / NT;
+    cx<T> v[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H4 * W4) {
+            const int ry = i / W4, rx = i - ry * W4;
+            v[k] = P.psi0[(long long)min(ty0 - 4 + ry, rmax) * pitch + min(tx0 - 4 + rx, cmax)];
+        }
     }
     // 2) pointwise values of the owned pairs; R3 pair (qy, qx..qx+1)
     cx<T> y0[OWN][2], acc[OWN][2];
@@ -208,6 +215,14 @@ __global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ F
             pu[j][h] = (RES && has_pump && own) ? __ldg(P.pump + g) : (T)0;
             po[j][h] = (has_pot && own) ? __ldg(P.pot + g) : (T)0;
             ns[j][h] = n0[j][h];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H4 * W4) {
+            const int ry = i / W4, rx = i - ry * W4;
+            sA[ry * SW + rx + 1] = v[k];
         }
     }
     __syncthreads();

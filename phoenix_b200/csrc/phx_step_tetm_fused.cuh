@@ -86,23 +86,53 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
     const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
     const int rmax = N_r + kRing - 1, cmax = N_c + kRing - 1;
 
-    // 1) psi0 of both components over tile + 4 into A; reservoirs over tile + 3
-    for (int i = threadIdx.x; i < H4 * W4; i += NT) {
-        const int ry = i / W4, rx = i - ry * W4;
-        const int gy = min(ty0 - 4 + ry, rmax), gx = min(tx0 - 4 + rx, cmax);
-        const long long g = (long long)gy * pitch + gx;
-        pbuf(0, 0)[ry * SW + rx + 1] = F.psi0[0][g];
-        pbuf(0, 1)[ry * SW + rx + 1] = F.psi0[1][g];
+    // 1) psi0 of both components over tile + 4 into A; reservoirs and the
+    // inputs of group 0 over tile + 3.  A thread issues all its loads before
+    // its first shared store, so that their latencies overlap (a load-store
+    // loop waits for each in turn).
+    constexpr int NL0 = (H4 * W4 + NT - 1) / NT, NL1 = (NR + NT - 1) / NT;
+    cx<T> vp[NL0], vm[NL0];
+#pragma unroll
+    for (int k = 0; k < NL0; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H4 * W4) {
+            const int ry = i / W4, rx = i - ry * W4;
+            const long long g = (long long)min(ty0 - 4 + ry, rmax) * pitch + min(tx0 - 4 + rx, cmax);
+            vp[k] = F.psi0[0][g];
+            vm[k] = F.psi0[1][g];
+        }
     }
-    for (int i = threadIdx.x; i < NR; i += NT) {
-        const int qy = i / W3, qx = i - qy * W3;
-        const int gy = min(ty0 - 3 + qy, rmax), gx = min(tx0 - 3 + qx, cmax);
-        const long long g = (long long)gy * pitch + gx;
-        const T a = __ldg(F.n0[0] + g), b = __ldg(F.n0[1] + g);
-        nv[i] = a, nv[NR + i] = b, nv[2 * NR + i] = a, nv[3 * NR + i] = b;
-        if (P0.noise.on) xis[i] = stage_xi(P0, ty0 - 3 + qy, tx0 - 3 + qx);
-        if (P0.n_pump > 0) tin[i] = __ldg(P0.pump + g), tin[NR + i] = __ldg(F.st[0].pump + g);
-        if (P0.n_pot > 0) tin[2 * NR + i] = __ldg(P0.pot + g), tin[3 * NR + i] = __ldg(F.st[0].pot + g);
+    T va[NL1], vb[NL1], vi[4][NL1];
+#pragma unroll
+    for (int k = 0; k < NL1; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < NR) {
+            const int qy = i / W3, qx = i - qy * W3;
+            const long long g = (long long)min(ty0 - 3 + qy, rmax) * pitch + min(tx0 - 3 + qx, cmax);
+            va[k] = __ldg(F.n0[0] + g), vb[k] = __ldg(F.n0[1] + g);
+            if (P0.n_pump > 0) vi[0][k] = __ldg(P0.pump + g), vi[1][k] = __ldg(F.st[0].pump + g);
+            if (P0.n_pot > 0) vi[2][k] = __ldg(P0.pot + g), vi[3][k] = __ldg(F.st[0].pot + g);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NL0; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H4 * W4) {
+            const int ry = i / W4, rx = i - ry * W4;
+            pbuf(0, 0)[ry * SW + rx + 1] = vp[k];
+            pbuf(0, 1)[ry * SW + rx + 1] = vm[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NL1; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < NR) {
+            const int qy = i / W3, qx = i - qy * W3;
+            nv[i] = va[k], nv[NR + i] = vb[k], nv[2 * NR + i] = va[k], nv[3 * NR + i] = vb[k];
+            if (P0.noise.on) xis[i] = stage_xi(P0, ty0 - 3 + qy, tx0 - 3 + qx);
+            if (P0.n_pump > 0) tin[i] = vi[0][k], tin[NR + i] = vi[1][k];
+            if (P0.n_pot > 0) tin[2 * NR + i] = vi[2][k], tin[3 * NR + i] = vi[3][k];
+        }
     }
     __syncthreads();
 
@@ -250,17 +280,43 @@ __global__ void __launch_bounds__(NT) rk4_scalar_general_kernel(const __grid_con
     const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
     const int rmax = N_r + kRing - 1, cmax = N_c + kRing - 1;
 
-    for (int i = threadIdx.x; i < H4 * W4; i += NT) {
-        const int ry = i / W4, rx = i - ry * W4;
-        const int gy = min(ty0 - 4 + ry, rmax), gx = min(tx0 - 4 + rx, cmax);
-        pbuf(0)[ry * SW + rx + 1] = F.psi0[(long long)gy * pitch + gx];
+    // psi0 over tile + 4, n0 over tile + 3: every load of a thread issued
+    // before its first shared store (latencies overlap)
+    constexpr int NL0 = (H4 * W4 + NT - 1) / NT, NL1 = (NR + NT - 1) / NT;
+    cx<T> vp[NL0];
+    T va[NL1];
+#pragma unroll
+    for (int k = 0; k < NL0; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H4 * W4) {
+            const int ry = i / W4, rx = i - ry * W4;
+            vp[k] = F.psi0[(long long)min(ty0 - 4 + ry, rmax) * pitch + min(tx0 - 4 + rx, cmax)];
+        }
     }
-    for (int i = threadIdx.x; i < NR; i += NT) {
-        const int qy = i / W3, qx = i - qy * W3;
-        const int gy = min(ty0 - 3 + qy, rmax), gx = min(tx0 - 3 + qx, cmax);
-        const T a = RES ? __ldg(F.n0 + (long long)gy * pitch + gx) : (T)0;
-        nv[i] = a, nv[NR + i] = a;
-        if (P0.noise.on) xis[i] = stage_xi(P0, ty0 - 3 + qy, tx0 - 3 + qx);
+#pragma unroll
+    for (int k = 0; k < NL1; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < NR) {
+            const int qy = i / W3, qx = i - qy * W3;
+            va[k] = RES ? __ldg(F.n0 + (long long)min(ty0 - 3 + qy, rmax) * pitch + min(tx0 - 3 + qx, cmax)) : (T)0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NL0; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < H4 * W4) {
+            const int ry = i / W4, rx = i - ry * W4;
+            pbuf(0)[ry * SW + rx + 1] = vp[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NL1; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < NR) {
+            const int qy = i / W3, qx = i - qy * W3;
+            nv[i] = va[k], nv[NR + i] = va[k];
+            if (P0.noise.on) xis[i] = stage_xi(P0, ty0 - 3 + qy, tx0 - 3 + qx);
+        }
     }
     __syncthreads();
 
