@@ -166,7 +166,8 @@ typedef struct {
     int64_t kernel_launches;        /* this library's kernels launched */
     int32_t launch_shape;           /* launch shape in use: 0-3 per-stage kernels, 4-7 the fused
                                        RK4 iteration (tile shapes), 8-13 its persistent TMA-fed
-                                       variants, -1 while the first iterations time them */
+                                       tile variants, 14 the TMA-fed column-strip walk, -1 while
+                                       the first iterations time them */
     int32_t reserved;
 } phx_step_info;
 

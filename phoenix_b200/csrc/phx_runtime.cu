@@ -35,6 +35,7 @@
 #include "phx_stage_tetm.cuh"
 #include "phx_step_fused.cuh"
 #include "phx_step_tma.cuh"
+#include "phx_step_stream.cuh"
 #include "phx_step_tetm_fused.cuh"
 #include "phx_rt.hpp"
 #include "phx_adjoint.cuh"
@@ -134,7 +135,7 @@ struct Engine final : EngineBase {
     static constexpr int kTuneIters = 3;   // consecutive iterations of one candidate per sample
     static constexpr double kTuneMargin = 0.03;  // a challenger must beat the incumbent by this fraction
     static constexpr int kFusedShape = kShapes;  // launch shapes 4-7: whole RK4 iteration in one kernel
-    static constexpr int kFusedShapes = 10;      // shapes 8-13: persistent TMA-fed variants
+    static constexpr int kFusedShapes = 11;      // shapes 8-13: persistent TMA-fed tiles, 14: column strips
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kShapes + kFusedShapes];
     static constexpr int kRingBlocks = 256;  // blocks of the ring-norm kernels (their partial-sum slots follow the stage kernels')
     static constexpr int kNormBlocks = 296;
@@ -257,7 +258,7 @@ struct Engine final : EngineBase {
 
     long long grid_x(long long c0, long long c1) const { return (c1 - c0 + 32 * CPT - 1) / (32 * CPT); }
     // autotuning candidates: the stage kernels' shapes 0-3, or, where the
-    // one-kernel iteration applies, its shapes 4-13 (the stage kernels, four
+    // one-kernel iteration applies, its shapes 4-14 (the stage kernels, four
     // launches and 236 B per point, never beat it there)
     int first_candidate() const { return fused_eligible_static() ? kFusedShape : 0; }
     int n_candidates() const { return fused_eligible_static() ? kFusedShapes : kShapes; }
@@ -763,6 +764,61 @@ struct Engine final : EngineBase {
         const int blocks = std::min(Q.n_tiles, tma_blocks_per_sm * sm_count);
         kern<<<blocks, NT, Lay::total, stream>>>(Q);
     }
+    // ---- column strips (phx_step_stream.cuh): a CTA walks down a segment of a
+    // TW-wide strip, TH rows per step
+    template <bool RES, int TW, int TH, int NT, int MINB, bool FMA>
+    void go_stream(const FusedParams<T>& F) {
+        using Lay = StreamLayout<T, TW, TH>;
+        auto kern = rk4_stream_kernel<T, RES, TW, TH, NT, MINB, FMA>;
+        int& blocks_per_sm = tma_blocks[reinterpret_cast<const void*>(kern)];
+        if (!blocks_per_sm) {
+            PHX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::total));
+            PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, NT, Lay::total));
+            if (blocks_per_sm < 1) fail(PHX_ERR_UNSUPPORTED, "column-strip iteration kernel does not fit on an SM");
+        }
+        if (!err_flag.p) err_flag.alloc(sizeof(int), stream);
+        if (!sm_count) PHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, P.device));
+        auto map_of = [&](const void* base, bool complex) -> const CUtensorMap& {
+            const auto key = std::make_tuple(base, complex, TW + 8, TH);
+            auto it = store_maps.find(key);
+            if (it == store_maps.end()) {
+                CUtensorMap m;
+                tensor_map(&m, const_cast<void*>(base), complex, TW + 8, TH);
+                it = store_maps.emplace(key, m).first;
+            }
+            return it->second;
+        };
+        StreamParams<T> Q;
+        std::memset(&Q, 0, sizeof(Q));
+        Q.f = F;
+        Q.psi_map = map_of(psi[0].p, true);
+        if (RES) Q.n_map = map_of(nres[0].p, false);
+        if (F.pump) Q.pump_map = map_of(pump[0].p, false);
+        if (F.pot) Q.pot_map = map_of(pot[0].p, false);
+        Q.has_pump = F.pump != nullptr;
+        Q.has_pot = F.pot != nullptr;
+        Q.err = static_cast<int*>(err_flag.p);
+        Q.wait_polls = wait_polls;
+        // segments: the fewest step times, counting a prologue step per
+        // segment and the waves of CTAs over the SMs
+        Q.strips = (N_c + TW - 1) / TW;
+        const int row_steps = (N_r + TH - 1) / TH;
+        const long long slots = (long long)blocks_per_sm * sm_count;
+        long long best = -1;
+        for (int per = 1; per <= row_steps; ++per) {
+            const int seg_steps = (row_steps + per - 1) / per;
+            const int segs = (row_steps + seg_steps - 1) / seg_steps;
+            const long long ctas = (long long)Q.strips * segs;
+            const long long cost = ((ctas + slots - 1) / slots) * (seg_steps + 1);
+            if (best < 0 || cost < best) {
+                best = cost;
+                Q.seg_steps = seg_steps;
+                Q.n_segs = (int)ctas;
+            }
+        }
+        const int blocks = (int)std::min<long long>(Q.n_segs, slots);
+        kern<<<blocks, NT, Lay::total, stream>>>(Q);
+    }
     void check_err_flag() {
         if (!err_flag.p) return;
         int v = 0;
@@ -788,6 +844,13 @@ struct Engine final : EngineBase {
             // 64 x 14: 1024^2 makes 1184 tiles, exactly four rounds of 296 CTAs
             // (64 x 16 leaves the fourth round half empty)
             case 9: go_tma<RES, 64, f32 ? 14 : 7, 384, 2, FMA>(F); return;
+            // column strips: FP32 64 wide, 12 rows per step; FP64 32 wide, 8 rows
+            case 10:
+                if constexpr (f32)
+                    go_stream<RES, 64, 12, 448, 2, FMA>(F);
+                else
+                    go_stream<RES, 32, 8, 160, 2, FMA>(F);
+                return;
             default: break;
         }
         switch (cur_shape() - kFusedShape) {

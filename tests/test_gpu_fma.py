@@ -44,7 +44,7 @@ def test_fma_results_do_not_depend_on_the_launch_shape(require_gpu, monkeypatch)
     n = 320  # not a multiple of the 64-wide tiles
     wl = _bench().workload(n)
     ref = None
-    for shape in range(4, 14):
+    for shape in range(4, 15):
         psi, nres, info = _run(n, "f32", True, 12, wl, shape, monkeypatch)
         assert info.launch_shape == shape
         if ref is None:

@@ -143,11 +143,11 @@ SHAPE_CASES = ["rk4_f64_zero", "rk4_f64_periodic", "rk4_f64_mixed_rect", "rk4_f3
                "rk4_f64_temporal", "rk4_f64_nores"]
 
 
-@pytest.mark.parametrize("shape", list(range(14)))
+@pytest.mark.parametrize("shape", list(range(15)))
 @pytest.mark.parametrize("name", SHAPE_CASES)
 def test_every_launch_shape_gives_identical_results(require_gpu, shape, name, monkeypatch):
     """The autotuner may pick any launch shape (0-3: one kernel per RK stage,
-    4-13: the whole RK4 iteration in one kernel); all of them must reproduce the
+    4-14: the whole RK4 iteration in one kernel); all of them must reproduce the
     reference bit for bit (the mask case through cuFFT: to 1e-12)."""
     monkeypatch.setenv("PHX_STAGE_SHAPE", str(shape))
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
@@ -174,7 +174,7 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
     n = 1024
     wl = B.workload(n)
     res = {}
-    for shape in (2,) + tuple(range(4, 14)):
+    for shape in (2,) + tuple(range(4, 15)):
         monkeypatch.setenv("PHX_STAGE_SHAPE", str(shape))
         sp = B.system(pb, n, "f32", 0)
         sp.fft_every = 1e12
@@ -186,7 +186,7 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
             info = s.run(25)
             assert info.launch_shape == shape
             res[shape] = (s.get_field("psi_plus"), s.get_field("n_plus"))
-    for shape in range(4, 14):
+    for shape in range(4, 15):
         np.testing.assert_array_equal(res[2][0], res[shape][0])
         np.testing.assert_array_equal(res[2][1], res[shape][1])
 
@@ -194,7 +194,7 @@ def test_fused_iteration_matches_stage_kernels_1024_fp32(require_gpu, monkeypatc
 @pytest.mark.parametrize("dtype", ["f32", "f64"])
 @pytest.mark.parametrize("px,py", [(True, False), (False, True), (True, True)])
 def test_tma_iterations_on_ragged_grids(require_gpu, monkeypatch, dtype, px, py):
-    """The persistent TMA iterations (shapes 8-13) on a grid whose sides are
+    """The persistent TMA iterations (shapes 8-14, 14 walking column strips) on a grid whose sides are
     multiples of no tile side (tiles reach past the grid, the TMA boxes past
     the planes): bit-identical to the stage kernels after 7 iterations, with
     periodic and zero boundaries."""
@@ -207,7 +207,7 @@ def test_tma_iterations_on_ragged_grids(require_gpu, monkeypatch, dtype, px, py)
     pot = 0.1 * rng.standard_normal((n_r, n_c))
     n0 = rng.random((n_r, n_c))
     res = {}
-    for shape in (2, 8, 9, 10, 11, 12, 13):
+    for shape in (2, 8, 9, 10, 11, 12, 13, 14):
         monkeypatch.setenv("PHX_STAGE_SHAPE", str(shape))
         sp = pb.SystemParameters(N_c=n_c, N_r=n_r, L_x=60.0, L_y=40.0, **B.PHYS, periodic_boundary_x=px,
                                  periodic_boundary_y=py, dtype=dtype, iterator="RK4", dt=0.01, t0=0.0, t_max=1e12,
@@ -221,7 +221,7 @@ def test_tma_iterations_on_ragged_grids(require_gpu, monkeypatch, dtype, px, py)
             info = s.run(7)
             assert info.launch_shape == shape
             res[shape] = (s.get_field("psi_plus"), s.get_field("n_plus"))
-    for shape in (8, 9, 10, 11, 12, 13):
+    for shape in (8, 9, 10, 11, 12, 13, 14):
         np.testing.assert_array_equal(res[2][0], res[shape][0])
         np.testing.assert_array_equal(res[2][1], res[shape][1])
 
@@ -248,7 +248,7 @@ def test_autotuning_across_every_shape_is_bit_identical(require_gpu, monkeypatch
             s.set_field("n_plus", np.zeros((n, n)))
             s.set_field("pump_plus", wl["pump"], 0)
             s.set_field("potential_plus", wl["potential"], 0)
-            info = s.run(200)  # 10 candidates x 6 rounds x 3 iterations of tuning, then more
+            info = s.run(240)  # 11 candidates x 6 rounds x 3 iterations of tuning, then more
             if shape is None:
                 assert info.launch_shape >= 0  # tuning finished within the run
             outs.append((s.get_field("psi_plus"), s.get_field("n_plus")))
@@ -270,7 +270,7 @@ def test_tuned_shape_is_remembered_per_configuration(require_gpu, monkeypatch):
         with pb.Solver(sp) as s:
             s.set_field("psi_plus", np.zeros((n, n)))
             first = s.run(1).launch_shape
-            last = s.run(199).launch_shape
+            last = s.run(239).launch_shape
         return first, last
 
     tuned = first_shape(192)[1]
@@ -296,10 +296,10 @@ def test_tuning_reports_medians_and_keeps_the_incumbent_within_margin(require_gp
         s.set_field("psi_plus", np.zeros((n, n)))
         assert s.tune_report() == {}
         k = B.tune(s)
-        assert k == 10 * 6 * 3
+        assert k == 11 * 6 * 3
         rep = s.tune_report()
         chosen = s.run(0).launch_shape
-    assert sorted(rep) == list(range(4, 14))
+    assert sorted(rep) == list(range(4, 15))
     assert all(v > 0 for v in rep.values())
     best = min(rep.values())
     assert rep[chosen] == best or (chosen == 10 and rep[10] <= best * 1.03)
