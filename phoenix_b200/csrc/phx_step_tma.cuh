@@ -209,10 +209,6 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
         const int slot = it & 1;
         const unsigned parity = (unsigned)((it >> 1) & 1);
         const int next = tile + gridDim.x;
-        if (threadIdx.x == 0) {
-            pending_next = next < n_tiles;
-            if (pending_next) issue(slot ^ 1, next);
-        }
         const TileRef<T> R = tile_of(tile);
         if constexpr (BATCH) {
             // the previous tile's reads of sP ended at its closing barrier
@@ -226,6 +222,15 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
         // (no issue slots spent spinning), which also orders the data thread 0
         // observed before their reads
         const bool ok = threadIdx.x == 0 ? mbar_wait_bounded(&bars[slot], parity, wait_polls) : true;
+        // the next tile's boxes go into the other slot once this tile's are in
+        // (its reads of that slot ended at the previous tile's closing
+        // barrier): at the start of a launch, when every CTA's first loads
+        // come from DRAM at once, the first tiles do not share the bandwidth
+        // with the second ones; later the current boxes have long arrived
+        if (threadIdx.x == 0) {
+            pending_next = ok && next < n_tiles;
+            if (pending_next) issue(slot ^ 1, next);
+        }
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicExch(err, 1);
