@@ -62,7 +62,7 @@ struct Dp45Params {
     int ring;   // add the reference-norm rings 1..6, and sum ring 7 of the state
     double* partials;  // per block (error, norm, ring 7)
     unsigned* ticket;  // blocks finished; the last one sums the partials and resets it to 0
-    double* result;    // (error, norm without ring 7, ring 7 of the state), FP64
+    double* result;    // (error, norm without ring 7, ring 7 of the state), FP64 (device or mapped host memory)
 };
 
 template <typename T, int TW, int TH>
@@ -438,6 +438,8 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
     block_reduce2<NT>(a, b2, red);
     block_reduce1<NT>(c, red7);
     if (threadIdx.x == 0) {
+        // result may be mapped host memory: the host reads it after the
+        // stream has synchronised, when the kernel's writes are visible
         P.result[0] = a;
         P.result[1] = b2;
         P.result[2] = c;

@@ -5,6 +5,8 @@
 // the fused RK4 iteration.
 #pragma once
 
+#include <cstring>
+
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
@@ -73,6 +75,23 @@ struct PinnedBuf {
         if (p) cudaFreeHost(p);
         p = nullptr;
         PHX_CUDA(cudaMallocHost(&p, n));
+    }
+};
+
+// Pinned host memory mapped into the device's address space: a kernel writes
+// it directly, the host reads it after synchronising the stream (no copy).
+struct MappedBuf {
+    void* p = nullptr;  // host address
+    void* d = nullptr;  // device address
+    ~MappedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void alloc(size_t n) {
+        if (p) cudaFreeHost(p);
+        p = d = nullptr;
+        PHX_CUDA(cudaHostAlloc(&p, n, cudaHostAllocMapped));
+        std::memset(p, 0, n);
+        PHX_CUDA(cudaHostGetDevicePointer(&d, p, 0));
     }
 };
 

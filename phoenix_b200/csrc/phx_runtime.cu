@@ -1359,6 +1359,11 @@ struct Engine final : EngineBase {
     // the fused kernel reads the state over tile + 7: periodic images must be
     // 7 deep, which the stage kernels (4 deep) do not leave behind
     bool state_images_deep = false;
+    // the attempt kernel writes its three sums straight into mapped host
+    // memory (no device-to-host copy per attempt); -1 unknown, 0 the device
+    // cannot map host memory (the sums then go through `result` and a copy)
+    MappedBuf dp45_sums;
+    int dp45_mapped = -1;
     bool dp45_fused_set = false;
     DevBuf dp45_ticket;  // blocks of a fused attempt that have finished (the last one resets it)
     static constexpr int kDpTW = 32, kDpTH = 16;
@@ -1420,7 +1425,13 @@ struct Engine final : EngineBase {
         if (!dp45_ticket.p) dp45_ticket.alloc(sizeof(unsigned), stream);  // zeroed; the kernel leaves it at 0
         Q.partials = reinterpret_cast<double*>(partials.p);
         Q.ticket = static_cast<unsigned*>(dp45_ticket.p);
-        Q.result = reinterpret_cast<double*>(result.p);
+        if (dp45_mapped < 0) {
+            int can = 0;
+            PHX_CUDA(cudaDeviceGetAttribute(&can, cudaDevAttrCanMapHostMemory, P.device));
+            dp45_mapped = can ? 1 : 0;
+            if (dp45_mapped) dp45_sums.alloc(4 * sizeof(double));
+        }
+        Q.result = dp45_mapped ? static_cast<double*>(dp45_sums.d) : reinterpret_cast<double*>(result.p);
         constexpr int MINB = sizeof(T) == 4 ? 2 : 1;
         using Lay = Dp45Layout<T, kDpTW, kDpTH>;
         auto kern = P.use_reservoir ? dp45_fused_kernel<T, true, kDpTW, kDpTH, kDpNT, MINB>
@@ -1470,9 +1481,11 @@ struct Engine final : EngineBase {
                 ++launches;
                 PHX_CUDA(cudaGetLastError());
             }
-            PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            const bool mapped = fused_attempt && dp45_mapped == 1;
+            if (!mapped)
+                PHX_CUDA(cudaMemcpyAsync(host_result.p, result.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
             PHX_CUDA(cudaStreamSynchronize(stream));
-            const double* r = static_cast<const double*>(host_result.p);
+            const double* r = static_cast<const double*>(mapped ? dp45_sums.p : host_result.p);
             double err = r[0], nrm = r[1];
             if (ref_norm) {
                 // the reference's buffer still holds, in its outermost halo ring,
