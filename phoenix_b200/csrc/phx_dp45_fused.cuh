@@ -235,8 +235,10 @@ __global__ void __launch_bounds__(NT, MINB) dp45_fused_kernel(const __grid_const
 
     // 3) stages 1..6; stage s covers margin s - 1 of the stage-1 region.  A
     // pair straddling the region's x edge computes both points; the outer one
-    // is stored but never read as a value the reference computes.
-#pragma unroll 1
+    // is stored but never read as a value the reference computes.  The stages
+    // are unrolled: each one's weight sums, k-stack offsets and region bounds
+    // become constants (93.6 against 106.7 us per attempt at 1024^2 FP32).
+#pragma unroll
     for (int s = 1; s <= 6; ++s) {
         const int m = s - 1;
         const cx<T>* in = (s & 1) ? sY0 : sY1;  // Y_s: stage 1 reads the state in sY0
