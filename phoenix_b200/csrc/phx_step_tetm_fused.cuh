@@ -138,8 +138,10 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
 
     // 2) stages: stage s evaluates tile + (3 - s); A -> B, B -> C, C -> B, B -> state.
     // One point per work item, items spread evenly over the threads; the
-    // point's accumulators and reservoirs live in shared memory.
-#pragma unroll 1
+    // point's accumulators and reservoirs live in shared memory.  The four
+    // stages are unrolled (their buffers, regions and sums become constants;
+    // the item loop inside stays rolled, four copies of the right-hand side).
+#pragma unroll
     for (int s = 0; s < 4; ++s) {
         const TetmParams<T>& Q = F.st[s];
         const StageParams<T>& P = Q.p;
@@ -320,7 +322,7 @@ __global__ void __launch_bounds__(NT) rk4_scalar_general_kernel(const __grid_con
     }
     __syncthreads();
 
-#pragma unroll 1
+#pragma unroll
     for (int s = 0; s < 4; ++s) {
         const StageParams<T>& P = F.st[s];
         const int ib = s == 0 ? 0 : (s == 2 ? 2 : 1), ob = s == 1 ? 2 : 1;
