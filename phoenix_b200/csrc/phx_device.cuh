@@ -58,6 +58,17 @@ __device__ __forceinline__ T abs2(cx<T> z) { return radd(rmul(z.re, z.re), rmul(
 template <typename T>
 __device__ __forceinline__ cx<T> cmul_general(cx<T> s, cx<T> z) { return cmul(s, z); }
 
+// Programmatic dependent launch (sm_90+): a kernel launched with the
+// programmatic stream serialization attribute may start while the kernel
+// before it in the stream drains; pdl_wait() returns once that kernel has
+// completed and its writes are visible, so it comes before the first read of
+// anything the previous kernel wrote (and before any write it could still
+// read).  pdl_trigger() lets the next such kernel be scheduled once every CTA
+// of this grid has issued it or exited.  Both do nothing in a kernel launched
+// without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Grid-point storage.  Every field is a halo-padded plane: interior point
 // (r, c), 0 <= r < N_r, 0 <= c < N_c, sits at base[r * pitch + c] where base
 // points at interior (0, 0); rows and columns -G .. N+G-1 are addressable.

@@ -26,6 +26,7 @@
 #include <mutex>
 #include <atomic>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "../../include/phx.h"
@@ -684,10 +685,35 @@ struct Engine final : EngineBase {
     // this iteration needs the per-stage kernels (complex temporal
     // coefficients).
     // fused-iteration tile shapes (TW x TH points, NT threads); FP64 uses half-height tiles
+    // The one-kernel iterations are launched with programmatic stream
+    // serialization: the next iteration's kernel is scheduled while this one
+    // drains and waits (pdl_wait, phx_device.cuh) for it to complete before
+    // reading the state.  PHX_PDL=0 launches them plainly.
+    static bool pdl_on() {
+        static const bool on = [] {
+            const char* e = std::getenv("PHX_PDL");
+            return !(e && e[0] == '0');
+        }();
+        return on;
+    }
+    template <typename... KArgs, typename... Args>
+    void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = pdl_on() ? 1 : 0;
+        PHX_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+    }
     template <bool RES, int TW, int TH, int NT, bool FMA>
     void go_fused_shape(const FusedParams<T>& F) {
         dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
-        rk4_fused_kernel<T, RES, TW, TH, NT, false, FMA><<<grid, NT, 0, stream>>>(F);
+        launch_pdl(rk4_fused_kernel<T, RES, TW, TH, NT, false, FMA>, grid, dim3(NT), 0, F);
     }
     // ---- TMA-fed persistent variant
     int sm_count = 0;
@@ -762,7 +788,7 @@ struct Engine final : EngineBase {
         prepare_tma<TW, TH>(Q, F);
         Q.n_tiles = Q.tiles_x * ((N_r + TH - 1) / TH);
         const int blocks = std::min(Q.n_tiles, tma_blocks_per_sm * sm_count);
-        kern<<<blocks, NT, Lay::total, stream>>>(Q);
+        launch_pdl(kern, dim3(blocks), dim3(NT), Lay::total, Q);
     }
     // ---- column strips (phx_step_stream.cuh): a CTA walks down a segment of a
     // TW-wide strip, TH rows per step
@@ -817,7 +843,7 @@ struct Engine final : EngineBase {
             }
         }
         const int blocks = (int)std::min<long long>(Q.n_segs, slots);
-        kern<<<blocks, NT, Lay::total, stream>>>(Q);
+        launch_pdl(kern, dim3(blocks), dim3(NT), Lay::total, Q);
     }
     void check_err_flag() {
         if (!err_flag.p) return;

@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(NT) rk4_fused_kernel(const __grid_constant__ F
     const long long pitch = P.pitch;
     const bool has_pump = P.pump != nullptr, has_pot = P.pot != nullptr;
     const int rmax = P.N_r + kRing - 1, cmax = P.N_c + kRing - 1;
+    pdl_wait();  // the previous iteration's kernel has completed
 
     // 1) psi0 over tile + 4 into sA; R4 point (ry, rx) at sA[ry * SW + rx + 1].
     // The loads (and those of the pointwise values below) are all issued

@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(NT, MINB) rk4_stream_kernel(const __grid_const
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
+    pdl_wait();  // the previous iteration's kernel has completed
     __syncthreads();
     unsigned phase = 0;  // bit t: parity of the next phase of ring third t's mbarrier
     // step m of a segment (m = 0: the prologue) has base row R + (m - 1) TH;

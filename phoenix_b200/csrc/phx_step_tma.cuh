@@ -200,6 +200,9 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
+    // the previous iteration's state (and the plane this one writes, which the
+    // previous one read) are settled only once its kernel has completed
+    pdl_wait();
     __syncthreads();
     int tile = blockIdx.x;
     if (threadIdx.x == 0 && tile < n_tiles) issue(0, tile);
@@ -231,6 +234,11 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
             pending_next = ok && next < n_tiles;
             if (pending_next) issue(slot ^ 1, next);
         }
+        // this CTA's last tile: the next iteration's kernel may be scheduled
+        // (every CTA of this persistent grid is resident already, so its CTAs
+        // only take the slots these leave; they wait in pdl_wait() for this
+        // grid to complete)
+        if (next >= n_tiles) pdl_trigger();
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicExch(err, 1);
