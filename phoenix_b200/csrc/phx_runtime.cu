@@ -2083,6 +2083,9 @@ struct Engine final : EngineBase {
         Q.err = static_cast<int*>(err_flag.p);
         Q.wait_polls = wait_polls;
         const int blocks = std::min(Q.n_tiles, blocks_per_sm * sm_count);
+        // the backward's recomputes run on a second stream beside the
+        // vector-Jacobian sweep: launched plainly, no CTA waits resident for a
+        // predecessor while the other stream could use its slot
         kern<<<blocks, NT, Lay::total, stream>>>(Q);
     }
     // the same in one launch: the fused iteration kernel that also stores the
