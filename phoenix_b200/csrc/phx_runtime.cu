@@ -963,7 +963,7 @@ struct Engine final : EngineBase {
             tetm_fused_set = true;
         }
         dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
-        kern<<<grid, NT, Lay::bytes, stream>>>(F);
+        launch_pdl(kern, grid, dim3(NT), Lay::bytes, F);
     }
     void step_rk4_tetm_fused() {
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};
@@ -1028,7 +1028,7 @@ struct Engine final : EngineBase {
             general_set = true;
         }
         dim3 grid((unsigned)((N_c + TW - 1) / TW), (unsigned)((N_r + TH - 1) / TH));
-        kern<<<grid, NT, Lay::bytes, stream>>>(F);
+        launch_pdl(kern, grid, dim3(NT), Lay::bytes, F);
     }
     void step_rk4_general() {
         const T cw[4] = {(T)0.0, (T)0.5, (T)0.5, (T)1.0};

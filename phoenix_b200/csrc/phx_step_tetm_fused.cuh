@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(NT) rk4_tetm_fused_kernel(const __grid_constan
     const int N_r = P0.N_r, N_c = P0.N_c;
     const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
     const int rmax = N_r + kRing - 1, cmax = N_c + kRing - 1;
+    pdl_wait();  // the previous iteration's kernel has completed
 
     // 1) psi0 of both components over tile + 4 into A; reservoirs and the
     // inputs of group 0 over tile + 3.  A thread issues all its loads before
@@ -281,6 +282,7 @@ __global__ void __launch_bounds__(NT) rk4_scalar_general_kernel(const __grid_con
     const int N_r = P0.N_r, N_c = P0.N_c;
     const int tx0 = blockIdx.x * TW, ty0 = blockIdx.y * TH;
     const int rmax = N_r + kRing - 1, cmax = N_c + kRing - 1;
+    pdl_wait();  // the previous iteration's kernel has completed
 
     // psi0 over tile + 4, n0 over tile + 3: every load of a thread issued
     // before its first shared store (latencies overlap)
