@@ -90,8 +90,15 @@ struct BatchEngine final : BatchBase {
     DevBuf err_flag;
     int sm_count = 0;
 
-    // autotuning: the first 2 * kBatchShapes iterations cycle through the
-    // shapes (results do not depend on the shape); the second round is timed
+    // autotuning: the first kBatchTuneRounds * kBatchShapes iterations cycle
+    // through the shapes (results do not depend on the shape).  The first
+    // round warms up; each later one gives a sample per shape, and the median
+    // sample ranks them.  The incumbent (32 x 32 tiles, 384 threads) is kept
+    // unless the fastest median beats it by more than kBatchTuneMargin, so
+    // that boxes whose timings differ by noise pick the same shape.
+    static constexpr int kBatchTuneRounds = 4;
+    static constexpr int kBatchIncumbent = 3;
+    static constexpr double kBatchTuneMargin = 0.03;
     int shape = -1, tune_step = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_ev[kBatchShapes];
     std::vector<cudaEvent_t> events;
@@ -285,24 +292,27 @@ struct BatchEngine final : BatchBase {
         tune_ev[sh].push_back({a, b});
         cur ^= 1;
         advance_clocks(1);
-        if (++tune_step < 2 * kBatchShapes) return;
+        if (++tune_step < kBatchTuneRounds * kBatchShapes) return;
         PHX_CUDA(cudaStreamSynchronize(stream));
-        float best = 1e30f;
-        int best_sh = 0;
+        double best = 1e30, med[kBatchShapes];
+        int best_sh = kBatchIncumbent;
         for (int s = 0; s < kBatchShapes; ++s) {
-            float ms = 1e30f;
+            std::vector<double> v;
             for (size_t i = 1; i < tune_ev[s].size(); ++i) {
                 float m = 0.f;
                 PHX_CUDA(cudaEventElapsedTime(&m, tune_ev[s][i].first, tune_ev[s][i].second));
-                ms = std::min(ms, m);
+                v.push_back(m);
             }
-            if (ms < best) best = ms, best_sh = s;
+            std::sort(v.begin(), v.end());
+            med[s] = v[v.size() / 2];
+            if (med[s] < best) best = med[s], best_sh = s;
             for (auto& pr : tune_ev[s]) {
                 events.push_back(pr.first);
                 events.push_back(pr.second);
             }
             tune_ev[s].clear();
         }
+        if (med[kBatchIncumbent] <= best * (1.0 + kBatchTuneMargin)) best_sh = kBatchIncumbent;
         shape = best_sh;
     }
     void capture(int start) {

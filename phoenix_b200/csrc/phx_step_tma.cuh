@@ -174,13 +174,22 @@ __device__ __forceinline__ void tma_tile_loop(const TileOf& tile_of, int n_tiles
 
     __shared__ FusedParams<T> sP;  // BATCH: this tile's parameters
 
+    // BATCH, thread 0: the psi map of the instance whose maps it acquired
+    // last.  An acquire orders the issuing thread's later uses of a map, so
+    // a run of tiles of one instance needs one (fencing the same maps again
+    // for every tile made a batch of one 1024^2 instance take 39.5 instead
+    // of 35.0 us per iteration).
+    const CUtensorMap* acquired = nullptr;
     auto issue = [&](int slot, int g) {
         const TileRef<T> R = tile_of(g);
         if constexpr (BATCH) {
-            tensormap_acquire(R.psi_map);
-            if (RES) tensormap_acquire(R.n_map);
-            if (RES && R.has_pump) tensormap_acquire(R.pump_map);
-            if (R.has_pot) tensormap_acquire(R.pot_map);
+            if (R.psi_map != acquired) {
+                tensormap_acquire(R.psi_map);
+                if (RES) tensormap_acquire(R.n_map);
+                if (RES && R.has_pump) tensormap_acquire(R.pump_map);
+                if (R.has_pot) tensormap_acquire(R.pot_map);
+                acquired = R.psi_map;
+            }
         }
         unsigned char* base = smem + slot * Lay::slot_bytes;
         const unsigned tx_bytes = (unsigned)Lay::psi_bytes + (unsigned)Lay::real_bytes * (RES ? 1u : 0u) +

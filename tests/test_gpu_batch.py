@@ -63,7 +63,7 @@ def test_batch_matches_oracle_bitwise(require_gpu, dtype):
     with pb.BatchSolver([pb.system_from_case(c) for c, _ in inst]) as b:
         for i, (c, f) in enumerate(inst):
             load_batch(b, i, c, f)
-        i1 = b.run(43)  # 10 tuning iterations, two 16-iteration graphs from plane 0, one single launch
+        i1 = b.run(43)  # 20 tuning iterations, one 16-iteration graph from plane 0, seven single launches
         i2 = b.run(37)  # graphs from plane 1
         assert i1.iterations == 43 and i2.iterations == 37
         assert i1.launch_shape in (0, 1, 2, 3, 4)
