@@ -107,10 +107,10 @@ struct TmaLayout {
 };
 
 // Order earlier generic-proxy writes of a tensor map in global memory before
-// its use by the tensor-map proxy (maps written by a host copy before the
-// launch need nothing more).
+// this thread's uses of it by the tensor-map proxy.  The maps are written by
+// a host copy, hence system scope.
 __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(m) : "memory");
 }
 
 // 16-byte shared-memory access to the point pair at an even index
@@ -409,7 +409,15 @@ struct BatchParams {
 
 template <typename T, bool RES, int TW, int TH, int NT, int MINB = 1, bool FMA = false>
 __global__ void __launch_bounds__(NT, MINB) rk4_batch_kernel(const __grid_constant__ BatchParams<T> B) {
+    // the loop's g = b + k * gridDim.x (CTA b's k-th tile) is remapped to
+    // tile b * q + min(b, r) + k (q, r: n_tiles / gridDim.x and remainder),
+    // a bijection on [0, n_tiles) under which every CTA walks a contiguous
+    // run of tiles, mostly of one instance, so that thread 0 seldom fences
+    // a new instance's tensor maps
+    const int q = B.n_tiles / (int)gridDim.x, r = B.n_tiles % (int)gridDim.x;
     auto tile_of = [&](int g) {
+        const int cta = g % (int)gridDim.x, k = g / (int)gridDim.x;
+        g = cta * q + min(cta, r) + k;
         const BatchInstance<T>& I = B.inst[__ldg(B.tile_inst + g)];
         TileRef<T> R;
         R.psi_map = &I.maps[B.dir][0];
