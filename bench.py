@@ -399,8 +399,9 @@ def run_sweep(pb, torch, count, steps, device):
             "sequential_wall_s_incl_setup": seq_wall,
             "speedup_vs_sequential": seq_ms / batch_ms,
             "bit_identical_instances": equal,
-            "note": "one batch launch per iteration (captured graphs of 16) vs 256 single-simulation handles "
-                    "run one after another; both device-timed over the same iterations"}
+            "note": f"one batch launch per iteration (captured graphs of 16) vs {count} single-simulation "
+                    "handles run one after another, each grid size's launch shape tuned beforehand; both "
+                    "device-timed over the same iterations"}
 
 
 def run_adjoint(pb, torch, device, iters=500, n=512):
