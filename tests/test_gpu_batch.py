@@ -89,6 +89,29 @@ def test_every_batch_tile_shape_matches_oracle(require_gpu, shape, monkeypatch):
             np.testing.assert_array_equal(b.get_field(i, "n_plus"), np.real(ref["n_plus"]))
 
 
+RAGGED = [(256, 256), (192, 160), (224, 96), (160, 200), (256, 128), (96, 256), (200, 200), (256, 192),
+          (128, 224), (176, 144), (240, 240), (144, 112)]
+
+
+@pytest.mark.parametrize("shape", [0, 1, 2, 3, 4])
+def test_every_batch_tile_shape_with_more_tiles_than_ctas(require_gpu, shape, monkeypatch):
+    """12 ragged instances with mixed boundaries: 445-859 tiles per shape, more than the
+    296 or 592 resident CTAs and not a multiple of them, so every CTA walks a run of
+    several tiles across instance borders; one 16-iteration graph and nine single
+    launches, bit-identical to the oracle."""
+    monkeypatch.setenv("PHX_BATCH_SHAPE", str(shape))
+    inst = [make_instance(500 + k, c, r, "f32", px=k % 2, py=(k // 2) % 2) for k, (c, r) in enumerate(RAGGED)]
+    with pb.BatchSolver([pb.system_from_case(c) for c, _ in inst]) as b:
+        for i, (c, f) in enumerate(inst):
+            load_batch(b, i, c, f)
+        info = b.run(25)
+        assert info.launch_shape == shape and info.kernel_launches == 25
+        for i, (c, f) in enumerate(inst):
+            ref, _ = O.run(c, f, max_steps=25)
+            np.testing.assert_array_equal(b.get_field(i, "psi_plus"), ref["psi_plus"], err_msg=f"instance {i} psi")
+            np.testing.assert_array_equal(b.get_field(i, "n_plus"), np.real(ref["n_plus"]), err_msg=f"instance {i} n")
+
+
 def test_batch_matches_single_solvers_ragged_fp32(require_gpu):
     """Sweep-shaped batch: grid sizes from {128, 256, 512, 1024}, pump 0.8-3.0x
     threshold, disorder 0.05-0.2 meV rms; each instance equals its own Solver."""
